@@ -1,0 +1,231 @@
+/* mdelast B200 path: C-ABI of libmdelast_cuda.so.
+ *
+ * This is the boundary that replaces the C++ force-and-integrator core behind mdelast's
+ * pybind11 module md_driver_module (src/md_driver_module.cpp:16-224). Every entry point
+ * takes plain pointers and sizes, returns an int status (MDELAST_OK or a negative
+ * MDELAST_ERR_*), and reports details through mdelast_last_error(). Quantities crossing
+ * this boundary are in the reference's CGS units (src/units.hpp:6-24): cm, g, s, erg,
+ * dyn, erg/cm^3; Voigt order xx yy zz yz xz xy (src/md_driver.hpp:23-24).
+ *
+ * The compute path runs on the GPU (sm_100a). A call that needs the GPU fails with
+ * MDELAST_ERR_NO_DEVICE when no CUDA device is usable; there is no CPU fallback.
+ */
+#ifndef MDELAST_H_
+#define MDELAST_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MDELAST_ABI_VERSION 1
+
+/* return codes */
+#define MDELAST_OK 0
+#define MDELAST_ERR_ARGUMENT (-1)    /* invalid argument: message in mdelast_last_error() */
+#define MDELAST_ERR_CUDA (-2)        /* a CUDA runtime call failed */
+#define MDELAST_ERR_NO_DEVICE (-3)   /* no usable CUDA device */
+#define MDELAST_ERR_FATAL (-4)       /* a physics check the reference ends the run on */
+#define MDELAST_ERR_UNSUPPORTED (-5) /* valid in the reference but not on this path */
+#define MDELAST_ERR_CAPACITY (-6)    /* a fixed capacity (neighbour slots, cell size) hit */
+
+/* Status bits of a driver (mdelast_observables.status). FATAL bits correspond to the
+ * reference's printf + exit(1) sites; WARN bits to its print-only sites. */
+#define MDELAST_FATAL_RHO_MAX 0x1u       /* eam.hpp:48-70: rho > rhomax_fatal */
+#define MDELAST_FATAL_VOLUME 0x2u        /* md_driver.cpp:493-497: volume jump > 5 % */
+#define MDELAST_FATAL_MOMENTUM 0x4u      /* md_driver.cpp:623-627 */
+#define MDELAST_FATAL_PRESSURE 0x8u      /* md_driver.cpp:693-698 */
+#define MDELAST_FATAL_CONSERVATION 0x10u /* md_driver.cpp:700-726 */
+#define MDELAST_ERR_LIST_OVERFLOW 0x20u  /* neighbour slots per atom exceeded */
+#define MDELAST_ERR_CELL_OVERFLOW 0x40u  /* atoms per cell exceeded */
+#define MDELAST_FATAL_MASK 0xffu
+#define MDELAST_WARN_VIRIAL 0x100u       /* md_driver.cpp:424-429 "FATAL VIRIALS" print */
+#define MDELAST_WARN_RMIN 0x200u         /* potential.hpp:93-95 r < rmin_fatal print */
+#define MDELAST_WARN_TCONF_ZERO 0x400u   /* md_driver.cpp:518-519 */
+
+/* enums of md_driver.hpp:20-21 */
+#define MDELAST_NVE 0
+#define MDELAST_NVT 1
+#define MDELAST_NPT 2
+#define MDELAST_NPT_FLEX 3
+#define MDELAST_THERMOSTAT_KINETIC 0
+#define MDELAST_THERMOSTAT_CONFIGURATIONAL 1
+#define MDELAST_THERMOSTAT_AVERAGE 2
+
+/* table interpolation (poly_table.hpp:137-176) */
+#define MDELAST_QUINTIC 0
+#define MDELAST_BSPLINE 1
+
+/* arithmetic of the pair kernels */
+#define MDELAST_PRECISION_FP64 0  /* FP64 throughout, CGS, the reference's formulas */
+#define MDELAST_PRECISION_MIXED 1 /* FP32 pair and table math, FP64 sums and integrator */
+
+const char *mdelast_last_error(void);
+int mdelast_abi_version(void);
+/* 1 when a CUDA device is usable, 0 otherwise (no error). */
+int mdelast_device_available(void);
+
+/* ---------------------------------------------------------------------------------
+ * Tabulated functions.
+ * mdelast_pair_table_create replaces the TablePotential constructor
+ * (potential.hpp:77-104, bound at md_driver_module.cpp:58-66); mdelast_eam_create the
+ * EAM constructor (eam.hpp:10-28, md_driver_module.cpp:68-85). Node arrays f, f', f''
+ * at x_i = i*h, i = 0..n-1, exactly as get_potential.py passes them. Coefficients are
+ * built once on the host in extended precision (poly_table.hpp:35-63) and uploaded when
+ * a driver is created. The host evaluators below serve the scalar calculate()/rho()/F()
+ * methods of the binding; the step itself never calls them.
+ * ------------------------------------------------------------------------------- */
+typedef struct mdelast_pair_s mdelast_pair;
+typedef struct mdelast_eam_s mdelast_eam;
+
+int mdelast_pair_table_create(double rcut, double rmin_fatal, double dr, int64_t n_nodes,
+                              const double *v, const double *dv, const double *d2v,
+                              int interpolation, mdelast_pair **out);
+/* Analytic pair potentials of potential.hpp:29-75 (Morse, LennardJones): host
+ * evaluation only; a driver given one returns MDELAST_ERR_UNSUPPORTED. */
+int mdelast_pair_morse_create(double rcut, double D, double alpha, double r0,
+                              mdelast_pair **out);
+int mdelast_pair_lj_create(double rcut, double epsilon, double sigma, mdelast_pair **out);
+/* Potential::calculate(r) (potential.hpp:16-26): out = {V, dV/dr, d2V/dr2}. */
+int mdelast_pair_eval(const mdelast_pair *p, double r, double out[3]);
+/* Parameters: rcut, rmin_fatal (tables), kind (0 table, 1 Morse, 2 LJ), interpolation */
+int mdelast_pair_info(const mdelast_pair *p, double *rcut, int *kind, int *interpolation);
+void mdelast_pair_destroy(mdelast_pair *p);
+
+int mdelast_eam_create(double rcut, double rhomax_fatal, double dr, double drho,
+                       int64_t n_r, const double *rho, const double *drho_dr,
+                       const double *d2rho_dr2, int64_t n_rho, const double *F,
+                       const double *dF, const double *d2F, int interpolation,
+                       mdelast_eam **out);
+/* EAM::rho, drhodr, d2rhodr2, F, dFdrho, d2Fdrho2 (eam.hpp:30-70) for what = 0..5.
+ * F-family calls with rho > rhomax_fatal return MDELAST_ERR_FATAL (the reference exits). */
+int mdelast_eam_eval(const mdelast_eam *e, int what, double x, double *out);
+int mdelast_eam_info(const mdelast_eam *e, double *rcut, double *rhomax_fatal,
+                     int *interpolation);
+void mdelast_eam_destroy(mdelast_eam *e);
+
+/* Evaluate a table on the GPU at n points (host arrays in and out; out is n x 3).
+ * which: 0 pair V/dV/d2V ; 1 rho/drho/d2rho ; 2 F/dF/d2F. Used to check the device
+ * table code against the host and the oracle. */
+int mdelast_table_eval_device(const mdelast_pair *p, const mdelast_eam *e, int which,
+                              const double *x, int64_t n, double *out);
+
+/* ---------------------------------------------------------------------------------
+ * Driver: one periodic cell, the state MDDriver holds (md_driver.hpp:18-168).
+ * mdelast_driver_create replaces the 17-argument MDDriver constructor
+ * (md_driver.cpp:16-160, md_driver_module.cpp:95-102) and, like it, builds the
+ * neighbour list (if enabled), computes forces, kinetic energies and thermodynamics.
+ * ------------------------------------------------------------------------------- */
+typedef struct mdelast_driver_s mdelast_driver;
+
+typedef struct {
+    int32_t n_atoms;
+    int32_t n_types;
+    const double *positions;  /* n_atoms x 3 [cm], |x| < box/2 (md_driver.cpp:91-97) */
+    const double *velocities; /* n_atoms x 3 [cm/s] */
+    const uint32_t *types;    /* n_atoms, < n_types */
+    const double *mass;       /* n_types [g] */
+    const mdelast_pair *const *pair; /* n_types (n_types+1)/2, slot j(j+1)/2 + i, i <= j */
+    const mdelast_eam *const *eam;   /* n_eam entries (0 or n_types) */
+    int32_t n_eam;
+    int32_t ensemble;         /* MDELAST_NVE .. */
+    int32_t coupling;         /* MDELAST_THERMOSTAT_* */
+    /* Thermostat(T, q, p_eta, Nf) (thermostat.hpp:9-38) */
+    double thermo_T;
+    int32_t thermo_nchain;
+    const double *thermo_q;
+    const double *thermo_p_eta;
+    double thermo_Nf;
+    /* Barostat(P, w, p_eps, Thermostat) (barostat.hpp:6-17) */
+    double baro_P;
+    double baro_w;
+    double baro_p_eps;
+    double baro_thermo_T;
+    int32_t baro_nchain;
+    const double *baro_q;
+    const double *baro_p_eta;
+    double baro_Nf;
+    double box[9];            /* Box.h, row major; must be diagonal */
+    int32_t n_rg;             /* g(r) bin centres (evenly spaced, rg[0] > 0) */
+    const double *rg;
+    double Nf;
+    double dt;
+    int32_t neighbors;        /* 1: Verlet list rebuilt by mdelast_driver_calculate_neighbors;
+                                 0: all pairs within the cutoff every force call */
+    double r_skin;            /* >= 1 */
+    double fatal_conservation;
+    int32_t precision;        /* MDELAST_PRECISION_* */
+    int32_t device;           /* CUDA device ordinal */
+} mdelast_driver_config;
+
+/* Scalar state and observables after the last step: the read-only attributes of
+ * MDDriver (md_driver_module.cpp:103-140). born_elasticity_tensor holds the upper
+ * triangle with zeros below the diagonal, as the reference stores it. */
+typedef struct {
+    double epot_eam_atom, epot_atom, ekin_atom, etot_atom;
+    double ekin_tot, etot_cons_initial, etot_cons, etot_cons_err;
+    double virial, total_laplacian, total_force2;
+    double temperature_kin, temperature_conf_inverse, pressure;
+    double time;
+    double cycle;
+    double born_stress_tensor[6];
+    double stress_tensor[6];
+    double born_elasticity_tensor[36];
+    double box[9];
+    double baro_epsilon, baro_p_epsilon;
+    double momentum_tot[3];
+    uint32_t status;
+    uint32_t sample_observables;
+} mdelast_observables;
+
+int mdelast_driver_create(const mdelast_driver_config *cfg, mdelast_driver **out);
+void mdelast_driver_destroy(mdelast_driver *d);
+
+/* MDDriver::integrate() (md_driver.cpp:563-601), n_steps times. Asynchronous: a FATAL
+ * condition raised by a step is returned by the next call that reads results, as
+ * MDELAST_ERR_FATAL with the reference's message in mdelast_last_error(). */
+int mdelast_driver_integrate(mdelast_driver *d, int32_t n_steps);
+/* MDDriver::calculate_neighbors() (md_driver.cpp:279-298) */
+int mdelast_driver_calculate_neighbors(mdelast_driver *d);
+/* the sample_observables flag (md_driver.hpp:163-167) */
+int mdelast_driver_set_sample_observables(mdelast_driver *d, int32_t flag);
+int mdelast_driver_get_sample_observables(const mdelast_driver *d, int32_t *flag);
+/* wait for queued work; returns MDELAST_ERR_FATAL if a step raised a FATAL bit */
+int mdelast_driver_synchronize(mdelast_driver *d);
+
+int mdelast_driver_get_observables(mdelast_driver *d, mdelast_observables *out);
+
+/* per-atom arrays (md_driver_module.cpp:103-109) */
+#define MDELAST_ATOM_POSITIONS 0   /* n x 3 */
+#define MDELAST_ATOM_COORDINATES 1 /* n x 3, scaled, not wrapped (md_driver.cpp:483-485) */
+#define MDELAST_ATOM_VELOCITIES 2  /* n x 3 */
+#define MDELAST_ATOM_FORCES 3      /* n x 3 */
+#define MDELAST_ATOM_RHO 4         /* n */
+#define MDELAST_ATOM_EPOT 5        /* n */
+#define MDELAST_ATOM_EKIN 6        /* n */
+int mdelast_driver_get_atoms(mdelast_driver *d, int32_t field, double *out);
+
+/* Thermostat chains (thermostat.hpp:9-38): which 0 particle thermostat, 1 barostat's.
+ * Writes nchain values to each non-NULL array. */
+int mdelast_driver_get_chain(mdelast_driver *d, int32_t which, double *q, double *p_eta,
+                             double *eta, int32_t *nchain);
+
+/* The half list in the reference's CSR form (md_driver.hpp:87-90): point[n+1] and, for
+ * each atom i, its partners j > i in ascending order. Copies at most cap entries and
+ * returns the total in *n_entries. MDELAST_ERR_UNSUPPORTED when lists are disabled. */
+int mdelast_driver_get_neighbors(mdelast_driver *d, int32_t *point, int32_t *neighbors,
+                                 int64_t cap, int64_t *n_entries);
+
+/* Pair correlation (md_driver.cpp:732-862): mode 0 calculate_pair_correlation,
+ * 1 calculate_pair_correlations, 2 calculate_partial_pair_correlation. gr has n_rg
+ * values, gr_partial n_types(n_types+1)/2 x n_rg. */
+int mdelast_driver_pair_correlation(mdelast_driver *d, int32_t mode);
+int mdelast_driver_get_gr(mdelast_driver *d, double *gr, double *gr_partial);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MDELAST_H_ */

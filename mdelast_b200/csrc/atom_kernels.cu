@@ -1,0 +1,715 @@
+// Atom-parallel kernels of one MD step: neighbour-list build, density + embedding pass,
+// force + closing-kick pass, opening kick + drift. One thread per atom slot; every
+// replica's slots form whole blocks, so a block's partial sums belong to one replica.
+// The full neighbour list makes the pair passes gather-only: no atomics, deterministic
+// results, and forces that are antisymmetric pair by pair to the last bit.
+#include "kernels.cuh"
+
+namespace mdelast {
+
+namespace {
+
+__device__ __forceinline__ void status_or(Replica *rep, unsigned bits) {
+    atomicOr(&rep->obs.status, bits);
+}
+
+// Block-wide sum of NS per-thread values into out[0..NS) (thread 0 writes), warp shuffles
+// then shared memory; deterministic for a fixed block size.
+template <int NS>
+__device__ __forceinline__ void block_sum_store(double (&v)[NS], double *out) {
+    __shared__ double sm[kBlock / 32][NS];
+    int const lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+        double x = v[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+            x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0)
+            sm[warp][k] = x;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < NS; k += blockDim.x) {
+        double s = 0.;
+#pragma unroll
+        for (int w = 0; w < kBlock / 32; ++w)
+            s += sm[w][k];
+        out[k] = s;
+    }
+}
+
+} // namespace
+
+// ------------------------------------------------------------------------------------
+// neighbour list (md_driver.cpp:279-298): every pair with the reference's min-image
+// |p|^2 <= (rcut r_skin)^2, found through a cell list with cells no smaller than the list
+// radius (or all pairs when a replica has fewer than 3 cells along an edge).
+
+__global__ void k_cell_bin(AtomsView A) {
+    int const i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n_pad)
+        return;
+    int const r = A.rep_of[i];
+    if (r < 0)
+        return;
+    Replica const &R = A.rep[r];
+    if (R.nc[0] == 0)
+        return;
+    double4 const c = A.crd[i];
+    double const w[3] = {c.x - nint_ref(c.x), c.y - nint_ref(c.y), c.z - nint_ref(c.z)};
+    int idx[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        int k = static_cast<int>(floor((w[a] + 0.5) * R.nc[a]));
+        idx[a] = k < 0 ? 0 : (k >= R.nc[a] ? R.nc[a] - 1 : k);
+    }
+    int const cell = R.cell_begin + (idx[2] * R.nc[1] + idx[1]) * R.nc[0] + idx[0];
+    int const pos = atomicAdd(&A.cell_count[cell], 1);
+    if (pos < A.cell_cap)
+        A.cell_atoms[static_cast<size_t>(cell) * A.cell_cap + pos] = i;
+    else
+        status_or(&A.rep[r], MDELAST_ERR_CELL_OVERFLOW);
+}
+
+// Order each cell's members by slot index (rank sort in shared memory), so that the list
+// and everything summed over it are deterministic.
+__global__ void k_cell_sort(AtomsView A) {
+    extern __shared__ int s_mem[];
+    int const cell = blockIdx.x;
+    int n = A.cell_count[cell];
+    if (n > A.cell_cap)
+        n = A.cell_cap;
+    if (threadIdx.x == 0)
+        atomicMax(&A.max_count[1], A.cell_count[cell]);
+    int *src = s_mem;
+    int *dst = A.cell_atoms + static_cast<size_t>(cell) * A.cell_cap;
+    for (int k = threadIdx.x; k < n; k += blockDim.x)
+        src[k] = dst[k];
+    __syncthreads();
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        int const v = src[k];
+        int rank = 0;
+        for (int m = 0; m < n; ++m)
+            rank += src[m] < v;
+        dst[rank] = v;
+    }
+}
+
+// One batch of up to 32 candidate partners j of atom i (one per lane): lanes with a hit
+// store j in the atom's row, j > i from slot 0 up and j < i from slot maxn-1 down, in
+// lane order, so the list is deterministic (cell stencil order, then slot order within a
+// cell, which k_cell_sort fixed). nu/nd count the stored entries (nu + nd <= maxn, so the
+// pair kernels never read an unwritten slot); total counts every partner found.
+__device__ __forceinline__ void nb_batch(AtomsView const &A, int i, int j, bool hit,
+                                         unsigned lane, int &nu, int &nd, int &total,
+                                         bool &full) {
+    bool const hu = hit && j > i, hd = hit && j < i;
+    unsigned const up = __ballot_sync(0xffffffffu, hu);
+    unsigned const dn = __ballot_sync(0xffffffffu, hd);
+    int const cu = __popc(up), cd = __popc(dn);
+    total += cu + cd;
+    if (full || nu + nd + cu + cd > A.maxn) {
+        full = true;
+        return;
+    }
+    unsigned const lt = (1u << lane) - 1u;
+    size_t const row = static_cast<size_t>(i) * A.maxn;
+    if (hu)
+        A.nbr[row + nu + __popc(up & lt)] = j;
+    if (hd)
+        A.nbr[row + (A.maxn - 1 - nd - __popc(dn & lt))] = j;
+    nu += cu;
+    nd += cd;
+}
+
+// One warp per atom slot; the lanes test 32 candidates at a time.
+__global__ void k_nbr_build(AtomsView A) {
+    unsigned const lane = threadIdx.x & 31u;
+    int const i = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (i >= A.n_pad)
+        return;
+    int const r = A.rep_of[i];
+    if (r < 0) {
+        if (lane == 0) {
+            A.n_up[i] = 0;
+            A.n_dn[i] = 0;
+        }
+        return;
+    }
+    Replica const &R = A.rep[r];
+    double4 const ci = A.crd[i];
+    double const hx = R.h[0], hy = R.h[1], hz = R.h[2];
+    double const rl2 = A.r_list_sq;
+    int nu = 0, nd = 0, total = 0;
+    bool full = false;
+    double px, py, pz;
+    if (R.nc[0] == 0) {
+        int const b = R.atom_begin, e = R.atom_begin + R.n_atoms;
+        for (int base = b; base < e; base += 32) {
+            int const j = base + static_cast<int>(lane);
+            bool hit = false;
+            if (j < e && j != i)
+                hit = min_image_r2(ci, A.crd[j], hx, hy, hz, px, py, pz) <= rl2;
+            nb_batch(A, i, j, hit, lane, nu, nd, total, full);
+        }
+    } else {
+        double const w[3] = {ci.x - nint_ref(ci.x), ci.y - nint_ref(ci.y), ci.z - nint_ref(ci.z)};
+        int idx[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            int k = static_cast<int>(floor((w[a] + 0.5) * R.nc[a]));
+            idx[a] = k < 0 ? 0 : (k >= R.nc[a] ? R.nc[a] - 1 : k);
+        }
+        for (int dz = -1; dz <= 1; ++dz) {
+            int const cz = (idx[2] + dz + R.nc[2]) % R.nc[2];
+            for (int dy = -1; dy <= 1; ++dy) {
+                int const cy = (idx[1] + dy + R.nc[1]) % R.nc[1];
+                for (int dx = -1; dx <= 1; ++dx) {
+                    int const cx = (idx[0] + dx + R.nc[0]) % R.nc[0];
+                    int const cell = R.cell_begin + (cz * R.nc[1] + cy) * R.nc[0] + cx;
+                    int n = A.cell_count[cell];
+                    if (n > A.cell_cap)
+                        n = A.cell_cap;
+                    int const *m = A.cell_atoms + static_cast<size_t>(cell) * A.cell_cap;
+                    for (int base = 0; base < n; base += 32) {
+                        int const k = base + static_cast<int>(lane);
+                        int const j = k < n ? m[k] : -1;
+                        bool hit = false;
+                        if (k < n && j != i)
+                            hit = min_image_r2(ci, A.crd[j], hx, hy, hz, px, py, pz) <= rl2;
+                        nb_batch(A, i, j, hit, lane, nu, nd, total, full);
+                    }
+                }
+            }
+        }
+    }
+    if (lane == 0) {
+        A.n_up[i] = nu;
+        A.n_dn[i] = nd;
+        if (total > A.maxn)
+            status_or(&A.rep[r], MDELAST_ERR_LIST_OVERFLOW);
+        atomicMax(&A.max_count[0], total);
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// Density pass (md_driver.cpp:195-277): rho_i = sum_j rho_{type j}(r_ij); on sampled
+// steps g_i = sum_j rho'_{type j}(r)/r p p^T (Voigt) and h_i = sum_j rho'_{type j}(r)/r p,
+// then F, F', F'' of rho_i. g and h are only needed in F''_i g_i g_i^T and F''_i |h_i|^2,
+// so those per-atom Born and Laplacian terms (md_driver.cpp:410-419) are formed here and
+// g, h are never stored.
+
+// TPA lanes (a power of two dividing 32) share one atom: lane `sub` takes the atom's list
+// entries sub, sub + TPA, ... and the per-atom sums are combined across the lanes with
+// shuffles. TPA > 1 gives a small cell enough threads to cover the GPU; a large batch of
+// replicas runs with TPA = 1. Every lane reaches the shuffles (padding lanes add zeros).
+template <int TPA> __device__ __forceinline__ double group_sum(double x) {
+#pragma unroll
+    for (int o = TPA / 2; o > 0; o >>= 1)
+        x += __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
+}
+
+__device__ __forceinline__ int list_slot(int kk, int nu, int maxn) {
+    return kk < nu ? kk : maxn - 1 - (kk - nu);
+}
+
+// Work split: the blocks of a pass are dealt out to the replicas (A.dblk_rep / fblk_rep);
+// block lb of a replica with nb blocks takes atom groups lb, lb + nb, ... of kBlock/TPA
+// atoms, so a block's partial sums belong to one replica and the block-wide reduction at
+// the end is paid once for several groups.
+template <bool OBS, int TPA>
+__global__ void __launch_bounds__(kBlock) k_density(AtomsView A, TablesView T) {
+    int const r = A.dblk_rep[blockIdx.x];
+    Replica const *R = A.rep + r;
+    int const lb = blockIdx.x - R->dblk_begin, nb = R->dblk_n;
+    int const apb = kBlock / TPA, sub = threadIdx.x % TPA;
+    int const n_slots = R->n_blocks * kBlock;
+    double const hx = R->h[0], hy = R->h[1], hz = R->h[2];
+    double acc[D_NSUM];
+#pragma unroll
+    for (int k = 0; k < D_NSUM; ++k)
+        acc[k] = 0.;
+    for (int a0 = lb * apb; a0 < n_slots; a0 += nb * apb) {
+    int const a = a0 + static_cast<int>(threadIdx.x) / TPA;
+    int const i = R->atom_begin + a;
+    bool const valid = a < R->n_atoms && T.has_eam;
+    double rho = 0.;
+    double g[6] = {0, 0, 0, 0, 0, 0}, hv[3] = {0, 0, 0};
+    double4 ci = make_double4(0., 0., 0., 0.);
+    if (valid) {
+        ci = A.crd[i];
+        int const ti = static_cast<int>(ci.w);
+        int const nu = A.n_up[i], ntot = nu + A.n_dn[i];
+        int const *row = A.nbr + static_cast<size_t>(i) * A.maxn;
+        for (int kk = sub; kk < ntot; kk += TPA) {
+            int const j = row[list_slot(kk, nu, A.maxn)];
+            double4 const cj = A.crd[j];
+            double px, py, pz;
+            double const r2 = min_image_r2(ci, cj, hx, hy, hz, px, py, pz);
+            if (r2 > T.r_cut_sq)
+                continue;
+            double const dr = sqrt(r2);
+            int const tj = static_cast<int>(cj.w);
+            if (dr > T.eam_rcut[tj])
+                continue;
+            double t;
+            int const k = tab_locate(dr, T.inv_hr, T.nri, t);
+            int const s = pair_slot(ti, tj);
+            int const off = (tj == (ti < tj ? ti : tj)) ? 6 : 12;
+            double c[6];
+            ld6(T.rb + (static_cast<size_t>(s) * T.nri + k) * 18 + off, c);
+            rho += tab_v(c, t);
+            if (OBS) {
+                double const ar = tab_d1(c, t, T.inv_hr) / dr;
+                double const ap[3] = {ar * px, ar * py, ar * pz};
+                g[0] += ap[0] * px;
+                g[1] += ap[1] * py;
+                g[2] += ap[2] * pz;
+                g[3] += ap[1] * pz;
+                g[4] += ap[0] * pz;
+                g[5] += ap[0] * py;
+                hv[0] += ap[0];
+                hv[1] += ap[1];
+                hv[2] += ap[2];
+            }
+        }
+    }
+    rho = group_sum<TPA>(rho);
+    if (OBS) {
+#pragma unroll
+        for (int a = 0; a < 6; ++a)
+            g[a] = group_sum<TPA>(g[a]);
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+            hv[a] = group_sum<TPA>(hv[a]);
+    }
+    if (valid && sub == 0) {
+        int const ti = static_cast<int>(ci.w);
+        // embedding function (eam.hpp:48-70); rho beyond rhomax_fatal ends the reference run
+        if (rho > T.rhomax[ti])
+            status_or(A.rep + r, MDELAST_FATAL_RHO_MAX);
+        double t;
+        int const k = tab_locate(rho, T.inv_hf, T.nfi, t);
+        double c[6];
+        ld6(T.Ft + (static_cast<size_t>(ti) * T.nfi + k) * 6, c);
+        double const F = tab_v(c, t), dF = tab_d1(c, t, T.inv_hf);
+        double const d2F = OBS ? tab_d2(c, t, T.inv_hf2) : 0.;
+        A.rho[i] = rho;
+        A.Fe[i] = F;
+        if (OBS)
+            A.dF2[i] = make_double2(dF, d2F);
+        else
+            A.dF2[i].x = dF;
+        acc[D_FSUM] += F;
+        if (OBS) {
+            int q = D_CB;
+#pragma unroll
+            for (int u = 0; u < 6; ++u)
+#pragma unroll
+                for (int v = u; v < 6; ++v)
+                    acc[q++] += d2F * g[u] * g[v];
+            acc[D_LAP] += d2F * (hv[0] * hv[0] + hv[1] * hv[1] + hv[2] * hv[2]);
+        }
+    }
+    }
+    block_sum_store<D_NSUM>(acc, A.pd + static_cast<size_t>(blockIdx.x) * D_NSUM);
+}
+
+// ------------------------------------------------------------------------------------
+// Force pass (md_driver.cpp:300-430) with the closing half kick of velocity Verlet fused
+// in (md_driver.cpp:433-452; KICK). Per pair, with X = (phi'' - phi'/r + EAM terms)/r^2:
+//   dE/dr = phi' + F'_i rho'_j + F'_j rho'_i,  F_i += -(dE/dr)/r p
+// Global sums (virial, Born stress, Born tensor, pair Laplacian) take each pair once, on
+// its j > i visit; the Born tensor is accumulated as the 15 distinct degree-4 monomials
+// X p_a p_b p_c p_d of which its 21 upper-triangle entries are made.
+
+template <bool OBS, bool KICK, int TPA>
+__global__ void __launch_bounds__(kBlock) k_force(AtomsView A, TablesView T) {
+    int const r = A.fblk_rep[blockIdx.x];
+    Replica const *R = A.rep + r;
+    int const lb = blockIdx.x - R->fblk_begin, nb = R->fblk_n;
+    int const apb = kBlock / TPA, sub = threadIdx.x % TPA;
+    int const n_slots = R->n_blocks * kBlock;
+    double const hx = R->h[0], hy = R->h[1], hz = R->h[2];
+    double acc[F_NSUM];
+#pragma unroll
+    for (int k = 0; k < F_NSUM; ++k)
+        acc[k] = 0.;
+    for (int a0 = lb * apb; a0 < n_slots; a0 += nb * apb) {
+    int const a = a0 + static_cast<int>(threadIdx.x) / TPA;
+    int const i = R->atom_begin + a;
+    bool const valid = a < R->n_atoms;
+    double fx = 0., fy = 0., fz = 0., epot = 0.;
+    double4 ci = make_double4(0., 0., 0., 0.);
+    if (valid) {
+        ci = A.crd[i];
+        int const ti = static_cast<int>(ci.w);
+        double2 const dFi2 = T.has_eam ? A.dF2[i] : make_double2(0., 0.);
+        double const dFi = dFi2.x, d2Fi = OBS ? dFi2.y : 0.;
+        int const nu = A.n_up[i], ntot = nu + A.n_dn[i];
+        int const *row = A.nbr + static_cast<size_t>(i) * A.maxn;
+        bool warn_rmin = false;
+        for (int kk = sub; kk < ntot; kk += TPA) {
+            bool const upper = kk < nu;
+            int const j = row[list_slot(kk, nu, A.maxn)];
+            double4 const cj = A.crd[j];
+            double px, py, pz;
+            double const r2 = min_image_r2(ci, cj, hx, hy, hz, px, py, pz);
+            if (r2 > T.r_cut_sq)
+                continue;
+            double const dr = sqrt(r2);
+            double const idr = 1. / dr;
+            int const tj = static_cast<int>(cj.w);
+            int const s = pair_slot(ti, tj);
+            double t;
+            int const k = tab_locate(dr, T.inv_hr, T.nri, t);
+            const double *bundle = T.rb + (static_cast<size_t>(s) * T.nri + k) * 18;
+            // TablePotential::calculate (potential.hpp:92-104)
+            double V = 0., dV = 0., d2V = 0.;
+            if (dr < T.pot_rmin[s])
+                warn_rmin = true;
+            if (!(dr > T.pot_rcut[s])) {
+                double c[6];
+                ld6(bundle, c);
+                V = tab_v(c, t);
+                dV = tab_d1(c, t, T.inv_hr);
+                if (OBS)
+                    d2V = tab_d2(c, t, T.inv_hr2);
+            }
+            double dedr = dV;
+            double X = 0., lap = 0.;
+            if (OBS) {
+                X = d2V - dV * idr;
+                lap = 2. * (d2V + 2. * dV * idr);
+            }
+            if (T.has_eam) {
+                // rho of the lower type at bundle offset 6, of the higher type at 12
+                int const oi = (ti <= tj) ? 6 : 12, oj = (ti < tj) ? 12 : 6;
+                double drho_i = 0., drho_j = 0., d2rho_i = 0., d2rho_j = 0.;
+                if (!(dr > T.eam_rcut[ti])) {
+                    double c[6];
+                    ld6(bundle + oi, c);
+                    drho_i = tab_d1(c, t, T.inv_hr);
+                    if (OBS)
+                        d2rho_i = tab_d2(c, t, T.inv_hr2);
+                }
+                if (!(dr > T.eam_rcut[tj])) {
+                    double c[6];
+                    ld6(bundle + oj, c);
+                    drho_j = tab_d1(c, t, T.inv_hr);
+                    if (OBS)
+                        d2rho_j = tab_d2(c, t, T.inv_hr2);
+                }
+                double2 const dFj2 = A.dF2[j];
+                double const dFj = dFj2.x;
+                // the two cross terms are rounded separately and added (commutative), so
+                // the i- and j-side evaluations of dE/dr are bitwise equal
+                dedr = __dadd_rn(dedr, __dadd_rn(__dmul_rn(dFi, drho_j), __dmul_rn(dFj, drho_i)));
+                if (OBS) {
+                    double const d2Fj = dFj2.y;
+                    lap += 2. * (dFj * (d2rho_i + 2. * drho_i * idr) +
+                                 dFi * (d2rho_j + 2. * drho_j * idr));
+                    lap += d2Fi * (drho_j * drho_j) + d2Fj * (drho_i * drho_i);
+                    X += dFi * (d2rho_j - drho_j * idr) + dFj * (d2rho_i - drho_i * idr);
+                }
+            }
+            double const sc = __dmul_rn(-dedr, idr);
+            fx += __dmul_rn(sc, px);
+            fy += __dmul_rn(sc, py);
+            fz += __dmul_rn(sc, pz);
+            epot += 0.5 * V;
+            if (upper) {
+                acc[F_VIRIAL] += dr * dedr;
+                double const xx = px * px, yy = py * py, zz = pz * pz;
+                double const yz = py * pz, xz = px * pz, xy = px * py;
+                double const w = dedr * idr;
+                acc[F_SIGMA + 0] += w * xx;
+                acc[F_SIGMA + 1] += w * yy;
+                acc[F_SIGMA + 2] += w * zz;
+                acc[F_SIGMA + 3] += w * yz;
+                acc[F_SIGMA + 4] += w * xz;
+                acc[F_SIGMA + 5] += w * xy;
+                if (OBS) {
+                    X *= idr * idr;
+                    double const Xxx = X * xx, Xyy = X * yy, Xzz = X * zz;
+                    acc[F_CB + 0] += Xxx * xx;  // x4
+                    acc[F_CB + 1] += Xyy * yy;  // y4
+                    acc[F_CB + 2] += Xzz * zz;  // z4
+                    acc[F_CB + 3] += Xxx * xy;  // x3y
+                    acc[F_CB + 4] += Xxx * xz;  // x3z
+                    acc[F_CB + 5] += Xyy * xy;  // xy3
+                    acc[F_CB + 6] += Xyy * yz;  // y3z
+                    acc[F_CB + 7] += Xzz * xz;  // xz3
+                    acc[F_CB + 8] += Xzz * yz;  // yz3
+                    acc[F_CB + 9] += Xxx * yy;  // x2y2
+                    acc[F_CB + 10] += Xxx * zz; // x2z2
+                    acc[F_CB + 11] += Xyy * zz; // y2z2
+                    acc[F_CB + 12] += Xxx * yz; // x2yz
+                    acc[F_CB + 13] += Xyy * xz; // xy2z
+                    acc[F_CB + 14] += Xzz * xy; // xyz2
+                    acc[F_LAP] += lap;
+                }
+            }
+        }
+        if (warn_rmin)
+            status_or(A.rep + r, MDELAST_WARN_RMIN);
+    }
+    fx = group_sum<TPA>(fx);
+    fy = group_sum<TPA>(fy);
+    fz = group_sum<TPA>(fz);
+    epot = group_sum<TPA>(epot);
+    if (valid && sub == 0) {
+        int const ti = static_cast<int>(ci.w);
+        if (T.has_eam)
+            epot += A.Fe[i];
+        size_t const np = A.n_pad;
+        A.frc[i] = fx;
+        A.frc[np + i] = fy;
+        A.frc[np + i + np] = fz;
+        A.epot[i] = epot;
+        double const m = T.mass[ti];
+        double vx = A.vel[i], vy = A.vel[np + i], vz = A.vel[2 * np + i];
+        if (KICK) {
+            // U2 (md_driver.cpp:446-449): v = v e + (c dt) F / m
+            double const e = R->e_kick, cdt = R->cdt_kick;
+            vx = vx * e + cdt * fx / m;
+            vy = vy * e + cdt * fy / m;
+            vz = vz * e + cdt * fz / m;
+            A.vel[i] = vx;
+            A.vel[np + i] = vy;
+            A.vel[2 * np + i] = vz;
+        }
+        acc[F_F2] += fx * fx + fy * fy + fz * fz;
+        acc[F_EKIN] += 0.5 * m * (vx * vx + vy * vy + vz * vz);
+        acc[F_MVV + 0] += m * vx * vx;
+        acc[F_MVV + 1] += m * vy * vy;
+        acc[F_MVV + 2] += m * vz * vz;
+        acc[F_MVV + 3] += m * vy * vz;
+        acc[F_MVV + 4] += m * vx * vz;
+        acc[F_MVV + 5] += m * vx * vy;
+        acc[F_MV + 0] += vx * m;
+        acc[F_MV + 1] += vy * m;
+        acc[F_MV + 2] += vz * m;
+        acc[F_EPOT] += epot;
+    }
+    }
+    block_sum_store<F_NSUM>(acc, A.pf + static_cast<size_t>(blockIdx.x) * F_NSUM);
+}
+
+// ------------------------------------------------------------------------------------
+// Opening half kick and drift (md_driver.cpp:433-499): the velocities first take the
+// thermostat factor of the preceding NHC half step (Replica::s_kick, which includes the
+// factor deferred from the previous step), then v = v e + (c dt) F / m, then
+// c += (cf dt) v / h with the box before this step's barostat update.
+
+__global__ void __launch_bounds__(kBlock) k_kick_drift(AtomsView A, TablesView T) {
+    int const i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n_pad)
+        return;
+    int const r = A.rep_of[i];
+    if (r < 0)
+        return;
+    Replica const *R = A.rep + r;
+    size_t const np = A.n_pad;
+    double4 c = A.crd[i];
+    double const m = T.mass[static_cast<int>(c.w)];
+    double const s = R->s_kick, e = R->e_kick, cdt = R->cdt_kick, a = R->cfdt;
+    double v[3] = {A.vel[i] * s, A.vel[np + i] * s, A.vel[2 * np + i] * s};
+    double const f[3] = {A.frc[i], A.frc[np + i], A.frc[2 * np + i]};
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        v[k] = v[k] * e + cdt * f[k] / m;
+    A.vel[i] = v[0];
+    A.vel[np + i] = v[1];
+    A.vel[2 * np + i] = v[2];
+    c.x = __dadd_rn(c.x, __ddiv_rn(__dmul_rn(a, v[0]), R->h_pos[0]));
+    c.y = __dadd_rn(c.y, __ddiv_rn(__dmul_rn(a, v[1]), R->h_pos[1]));
+    c.z = __dadd_rn(c.z, __ddiv_rn(__dmul_rn(a, v[2]), R->h_pos[2]));
+    A.crd[i] = c;
+}
+
+// ------------------------------------------------------------------------------------
+// Readout of one per-atom field in the C-ABI layout (x, y, z interleaved per atom) for
+// replica r, applying the deferred velocity factor.
+
+__global__ void k_readout(AtomsView A, TablesView T, int r, int field, double *out,
+                          const double *pos0, int stepped) {
+    Replica const *R = A.rep + r;
+    int const n = R->n_atoms;
+    int const a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n)
+        return;
+    int const i = R->atom_begin + a;
+    size_t const np = A.n_pad;
+    switch (field) {
+    case MDELAST_ATOM_POSITIONS: {
+        if (!stepped) {
+            out[3 * a] = pos0[3 * a];
+            out[3 * a + 1] = pos0[3 * a + 1];
+            out[3 * a + 2] = pos0[3 * a + 2];
+        } else {
+            double4 const c = A.crd[i];
+            out[3 * a] = __dmul_rn(__dadd_rn(c.x, -nint_ref(c.x)), R->h_pos[0]);
+            out[3 * a + 1] = __dmul_rn(__dadd_rn(c.y, -nint_ref(c.y)), R->h_pos[1]);
+            out[3 * a + 2] = __dmul_rn(__dadd_rn(c.z, -nint_ref(c.z)), R->h_pos[2]);
+        }
+        break;
+    }
+    case MDELAST_ATOM_COORDINATES: {
+        double4 const c = A.crd[i];
+        out[3 * a] = c.x;
+        out[3 * a + 1] = c.y;
+        out[3 * a + 2] = c.z;
+        break;
+    }
+    case MDELAST_ATOM_VELOCITIES:
+        out[3 * a] = A.vel[i] * R->vscale;
+        out[3 * a + 1] = A.vel[np + i] * R->vscale;
+        out[3 * a + 2] = A.vel[2 * np + i] * R->vscale;
+        break;
+    case MDELAST_ATOM_FORCES:
+        out[3 * a] = A.frc[i];
+        out[3 * a + 1] = A.frc[np + i];
+        out[3 * a + 2] = A.frc[2 * np + i];
+        break;
+    case MDELAST_ATOM_RHO:
+        out[a] = A.rho[i];
+        break;
+    case MDELAST_ATOM_EPOT:
+        out[a] = A.epot[i];
+        break;
+    case MDELAST_ATOM_EKIN: {
+        double const m = T.mass[static_cast<int>(A.crd[i].w)];
+        double const vx = A.vel[i] * R->vscale, vy = A.vel[np + i] * R->vscale,
+                     vz = A.vel[2 * np + i] * R->vscale;
+        out[a] = 0.5 * m * (vx * vx + vy * vy + vz * vz);
+        break;
+    }
+    default:
+        break;
+    }
+}
+
+// The reference-format half list of replica r: for each atom its partners j > i, in
+// ascending order (md_driver.cpp:283-294). counts[a] = n_up of atom a (pass 1) and the
+// sorted entries written at point[a] (pass 2).
+__global__ void k_half_list_counts(AtomsView A, int r, int *counts) {
+    Replica const *R = A.rep + r;
+    int const a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= R->n_atoms)
+        return;
+    counts[a] = A.n_up[R->atom_begin + a];
+}
+
+__global__ void k_half_list_fill(AtomsView A, int r, const int *point, int *out) {
+    Replica const *R = A.rep + r;
+    int const a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= R->n_atoms)
+        return;
+    int const i = R->atom_begin + a;
+    int const n = A.n_up[i];
+    int *o = out + point[a];
+    for (int k = 0; k < n; ++k)
+        o[k] = A.nbr[static_cast<size_t>(i) * A.maxn + k] - R->atom_begin;
+    for (int k = 1; k < n; ++k) { // insertion sort of a short run
+        int const v = o[k];
+        int m = k - 1;
+        while (m >= 0 && o[m] > v) {
+            o[m + 1] = o[m];
+            --m;
+        }
+        o[m + 1] = v;
+    }
+}
+
+__global__ void k_status_and(AtomsView A, unsigned mask) {
+    for (int r = threadIdx.x; r < A.n_rep; r += blockDim.x)
+        atomicAnd(&A.rep[r].obs.status, mask);
+}
+
+// Table values on the device for the table checks: which 0 pair slot s, 1 rho of type s,
+// 2 F of type s. Same code paths as the pair kernels.
+__global__ void k_table_eval(TablesView T, int which, int s, const double *x, int n,
+                             double *out) {
+    int const q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n)
+        return;
+    double const xv = x[q];
+    double t, c[6];
+    double v[3] = {0., 0., 0.};
+    if (which == 2) {
+        int const k = tab_locate(xv, T.inv_hf, T.nfi, t);
+        ld6(T.Ft + (static_cast<size_t>(s) * T.nfi + k) * 6, c);
+        v[0] = tab_v(c, t);
+        v[1] = tab_d1(c, t, T.inv_hf);
+        v[2] = tab_d2(c, t, T.inv_hf2);
+    } else {
+        int const k = tab_locate(xv, T.inv_hr, T.nri, t);
+        int slot, off;
+        double rc;
+        if (which == 0) {
+            slot = s;
+            off = 0;
+            rc = T.pot_rcut[s];
+        } else {
+            slot = pair_slot(s, s);
+            off = 6;
+            rc = T.eam_rcut[s];
+        }
+        if (!(xv > rc)) {
+            ld6(T.rb + (static_cast<size_t>(slot) * T.nri + k) * 18 + off, c);
+            v[0] = tab_v(c, t);
+            v[1] = tab_d1(c, t, T.inv_hr);
+            v[2] = tab_d2(c, t, T.inv_hr2);
+        }
+    }
+    out[3 * q] = v[0];
+    out[3 * q + 1] = v[1];
+    out[3 * q + 2] = v[2];
+}
+
+namespace {
+template <bool OBS> void density_tpa(int tpa, int grid, cudaStream_t s, AtomsView const &A,
+                                     TablesView const &T) {
+    switch (tpa) {
+    case 1: k_density<OBS, 1><<<grid, kBlock, 0, s>>>(A, T); break;
+    case 4: k_density<OBS, 4><<<grid, kBlock, 0, s>>>(A, T); break;
+    case 8: k_density<OBS, 8><<<grid, kBlock, 0, s>>>(A, T); break;
+    default: k_density<OBS, 16><<<grid, kBlock, 0, s>>>(A, T); break;
+    }
+}
+template <bool OBS, bool KICK>
+void force_tpa(int tpa, int grid, cudaStream_t s, AtomsView const &A, TablesView const &T) {
+    switch (tpa) {
+    case 1: k_force<OBS, KICK, 1><<<grid, kBlock, 0, s>>>(A, T); break;
+    case 4: k_force<OBS, KICK, 4><<<grid, kBlock, 0, s>>>(A, T); break;
+    case 8: k_force<OBS, KICK, 8><<<grid, kBlock, 0, s>>>(A, T); break;
+    default: k_force<OBS, KICK, 16><<<grid, kBlock, 0, s>>>(A, T); break;
+    }
+}
+} // namespace
+
+bool valid_tpa(int tpa) { return tpa == 1 || tpa == 4 || tpa == 8 || tpa == 16; }
+
+void launch_density(bool obs, int tpa, int grid, cudaStream_t s, AtomsView const &A,
+                    TablesView const &T) {
+    if (obs)
+        density_tpa<true>(tpa, grid, s, A, T);
+    else
+        density_tpa<false>(tpa, grid, s, A, T);
+}
+
+void launch_force(bool obs, bool kick, int tpa, int grid, cudaStream_t s, AtomsView const &A,
+                  TablesView const &T) {
+    if (obs && kick)
+        force_tpa<true, true>(tpa, grid, s, A, T);
+    else if (obs)
+        force_tpa<true, false>(tpa, grid, s, A, T);
+    else if (kick)
+        force_tpa<false, true>(tpa, grid, s, A, T);
+    else
+        force_tpa<false, false>(tpa, grid, s, A, T);
+}
+
+} // namespace mdelast

@@ -1,0 +1,173 @@
+// Device-side layout of the mdelast B200 path: per-replica state, the atom arrays in HBM,
+// and the inline helpers shared by the kernels.
+//
+// Layout (all arrays padded so that every replica starts on a multiple of kTile slots and
+// no thread block straddles two replicas):
+//   crd   double4[n_pad]   scaled coordinates (not wrapped, as md_driver.cpp:483-485 keeps
+//                          them) and the type in .w - the one record a pair gather reads
+//   vel   double[3][n_pad] velocities (SoA), times Replica::vscale (deferred NHC factor)
+//   frc   double[3][n_pad] forces
+//   rho, Fe, epot double[n_pad]; dF2 double2[n_pad] = (F'(rho), F''(rho))
+//   nbr   int[maxn][n_pad] full neighbour list, slot-major for coalesced index loads:
+//                          partners j > i from slot 0 up (n_up), j < i from maxn-1 down
+//   rb    double[npot][nri][18] r-table bundle of each type pair (a <= b):
+//                          phi_ab | rho_a | rho_b quintic coefficients of one interval
+//   Ft    double[ntypes][nfi][6] embedding-function coefficients
+#pragma once
+
+#include <cstdint>
+
+#include "mdelast.h"
+
+namespace mdelast {
+
+constexpr int kMaxChain = 16;
+constexpr int kTile = 256;  // replica atom ranges start on multiples of kTile slots
+constexpr int kBlock = 128; // threads per block of the atom kernels (divides kTile)
+constexpr int kMaxTypes = 8;
+
+// Slots of the per-block partial sums of the force pass.
+enum FSlot : int {
+    F_VIRIAL = 0,  // sum dr * dE/dr over pairs
+    F_SIGMA = 1,   // 6 Born-stress components
+    F_CB = 7,      // 15 degree-4 monomials of X_ij dp (pair part of the Born tensor)
+    F_LAP = 22,    // pair part of the Laplacian
+    F_F2 = 23,     // sum |F_i|^2
+    F_EKIN = 24,   // sum m v^2 / 2 after the closing kick
+    F_MVV = 25,    // 6 components of sum m v_a v_b
+    F_MV = 31,     // 3 components of sum m v
+    F_EPOT = 34,   // sum of per-atom potential energies
+    F_NSUM = 35
+};
+// Slots of the per-block partial sums of the density pass.
+enum DSlot : int {
+    D_FSUM = 0, // sum of embedding energies F(rho_i)
+    D_CB = 1,   // 21 upper-triangle entries of F''_i g_i g_i^T
+    D_LAP = 22, // sum F''_i |h_i|^2
+    D_NSUM = 23
+};
+
+struct Chain {
+    double T, Nf;
+    int n, pad;
+    double q[kMaxChain], inv_q[kMaxChain], p_eta[kMaxChain], eta[kMaxChain];
+};
+
+struct Replica {
+    // set at creation
+    int atom_begin, n_atoms, block_begin, n_blocks; // slots [atom_begin, + n_blocks*kBlock)
+    int dblk_begin, dblk_n, fblk_begin, fblk_n;     // blocks of the density / force pass
+    int ensemble, coupling;
+    int cell_begin, nc[3]; // cells per dimension for the list build (nc[0] == 0: all pairs)
+    double Nf, alpha, dt, fatal_conservation, mass0;
+    double baro_P, baro_w;
+    double h0[3];
+    // evolving scalar state
+    double h[3];      // current box diagonal
+    double h_pos[3];  // box the positions array refers to (before the last U1 box update)
+    double eps, p_eps;
+    double vscale;    // pending uniform factor of the stored velocities
+    double s_kick, e_kick, cdt_kick, cfdt; // coefficients of this step's kick and drift
+    double etot_cons_initial;
+    double time, cycle;
+    Chain th, bth;
+    mdelast_observables obs;
+    int initialised, pad2;
+};
+
+struct TablesView {
+    const double *rb; // [npot][nri][18]
+    int nri, npot;
+    double inv_hr, inv_hr2;
+    const double *Ft; // [ntypes][nfi][6]
+    int nfi, ntypes;
+    double inv_hf, inv_hf2;
+    int has_eam, pad;
+    double r_cut_sq; // pow<2>(pot[0]->rcut), md_driver.cpp:42
+    double pot_rcut[kMaxTypes * (kMaxTypes + 1) / 2];
+    double pot_rmin[kMaxTypes * (kMaxTypes + 1) / 2];
+    double eam_rcut[kMaxTypes];
+    double rhomax[kMaxTypes];
+    double mass[kMaxTypes];
+};
+
+struct AtomsView {
+    int n_pad, n_rep;
+    Replica *rep;
+    const int *rep_of; // replica of each slot, -1 for padding
+    double4 *crd;
+    double *vel, *frc; // [3][n_pad]
+    double *rho, *Fe, *epot;
+    double2 *dF2;
+    int *nbr, *n_up, *n_dn;
+    int maxn;
+    double *pd, *pf; // per-block partial sums [n_blocks][D_NSUM], [n_blocks][F_NSUM]
+    const int *dblk_rep, *fblk_rep; // replica of each block of the density / force pass
+    // cell list (list builds)
+    int *cell_count, *cell_atoms;
+    int cell_cap, n_cells;
+    double r_list_sq;
+    int *max_count; // [2]: largest neighbour count, largest cell count of the last build
+};
+
+// md_driver.hpp:48-50: round half away from zero through a truncating int conversion
+__device__ __forceinline__ double nint_ref(double x) {
+    return static_cast<double>(x < 0. ? static_cast<int>(__dadd_rn(x, -0.5))
+                                      : static_cast<int>(__dadd_rn(x, 0.5)));
+}
+
+// md_driver.cpp:175-185 with the reference's exact operations (no contraction):
+// p = (d - nint(d)) * h for d = ci - cj, and r2 = (px*px + py*py) + pz*pz.
+__device__ __forceinline__ double min_image_r2(double4 ci, double4 cj, double hx, double hy,
+                                               double hz, double &px, double &py, double &pz) {
+    double dx = __dadd_rn(ci.x, -cj.x), dy = __dadd_rn(ci.y, -cj.y), dz = __dadd_rn(ci.z, -cj.z);
+    dx = __dadd_rn(dx, -nint_ref(dx));
+    dy = __dadd_rn(dy, -nint_ref(dy));
+    dz = __dadd_rn(dz, -nint_ref(dz));
+    px = __dmul_rn(dx, hx);
+    py = __dmul_rn(dy, hy);
+    pz = __dmul_rn(dz, hz);
+    return __dadd_rn(__dadd_rn(__dmul_rn(px, px), __dmul_rn(py, py)), __dmul_rn(pz, pz));
+}
+
+__host__ __device__ __forceinline__ int pair_slot(int a, int b) {
+    int const hi = a > b ? a : b, lo = a > b ? b : a;
+    return hi * (hi + 1) / 2 + lo;
+}
+
+// poly_table.hpp:105-114: interval index clamped in floating point, local coordinate t.
+__device__ __forceinline__ int tab_locate(double x, double inv_h, int n, double &t) {
+    double const u = __dmul_rn(x, inv_h);
+    int i = 0;
+    if (u >= static_cast<double>(n))
+        i = n - 1;
+    else if (u > 0.)
+        i = static_cast<int>(u);
+    t = __dadd_rn(u, -static_cast<double>(i));
+    return i;
+}
+
+// Horner forms of poly_table.hpp:71-97 on the 6 coefficients c of one interval.
+__device__ __forceinline__ double tab_v(const double *c, double t) {
+    return c[0] + t * (c[1] + t * (c[2] + t * (c[3] + t * (c[4] + t * c[5]))));
+}
+__device__ __forceinline__ double tab_d1(const double *c, double t, double inv_h) {
+    return (c[1] + t * (2. * c[2] + t * (3. * c[3] + t * (4. * c[4] + t * 5. * c[5])))) * inv_h;
+}
+__device__ __forceinline__ double tab_d2(const double *c, double t, double inv_h2) {
+    return (2. * c[2] + t * (6. * c[3] + t * (12. * c[4] + t * 20. * c[5]))) * inv_h2;
+}
+
+// load the 6 coefficients of one interval (16-byte aligned) through the read-only path
+__device__ __forceinline__ void ld6(const double *p, double c[6]) {
+    const double2 *q = reinterpret_cast<const double2 *>(p);
+    double2 a = __ldg(q), b = __ldg(q + 1), d = __ldg(q + 2);
+    c[0] = a.x;
+    c[1] = a.y;
+    c[2] = b.x;
+    c[3] = b.y;
+    c[4] = d.x;
+    c[5] = d.y;
+}
+
+} // namespace mdelast

@@ -1,0 +1,906 @@
+// Host orchestration of the B200 path: the mdelast_driver_* entry points of
+// include/mdelast.h. A driver owns its device buffers and one stream; integrate() is one
+// CUDA-graph launch per step (the two graphs differ in whether the step samples the Born
+// tensor and the Laplacian). Results come back lazily: the graph's last node copies the
+// scalar observables into pinned host memory and the first read after a step waits for it.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "host_tables.h"
+#include "kernels.cuh"
+
+using namespace mdelast;
+
+#define CK(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            return fail(MDELAST_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_),    \
+                        __FILE__, __LINE__);                                                  \
+    } while (0)
+
+namespace {
+
+template <typename T> int dalloc(T **p, size_t n) {
+    CK(cudaMalloc(reinterpret_cast<void **>(p), sizeof(T) * (n > 0 ? n : 1)));
+    CK(cudaMemset(*p, 0, sizeof(T) * (n > 0 ? n : 1)));
+    return MDELAST_OK;
+}
+
+template <typename T> void dfree(T *&p) {
+    if (p)
+        cudaFree(p);
+    p = nullptr;
+}
+
+double nint_host(double x) { // md_driver.hpp:48-50
+    return static_cast<double>(x < 0. ? static_cast<int>(x - 0.5) : static_cast<int>(x + 0.5));
+}
+
+// Lanes per atom for the pair passes: the fewest that give about 150k threads (enough to
+// cover 148 SMs with the warps the register budget allows), at most 16. MDELAST_TPA
+// overrides it.
+int default_tpa(int n_atoms) {
+    if (char const *e = std::getenv("MDELAST_TPA")) {
+        int const v = std::atoi(e);
+        if (valid_tpa(v))
+            return v;
+    }
+    for (int t : {1, 4, 8})
+        if (static_cast<long>(n_atoms) * t >= 150000)
+            return t;
+    return 16;
+}
+
+// Deal the blocks of a pair pass out to the replicas in proportion to their atom counts:
+// about kTargetBlocks in all (a few resident waves on 148 SMs), never fewer than one per
+// replica nor more than one per atom group of kBlock/tpa atoms. Fills each replica's block
+// range and the block -> replica map; returns the grid size.
+constexpr int kTargetBlocks = 148 * 4;
+
+int deal_blocks(std::vector<Replica *> const &reps, int tpa, bool density,
+                std::vector<int> &blk_rep) {
+    long total = 0;
+    for (Replica const *r : reps)
+        total += r->n_blocks;
+    blk_rep.clear();
+    for (size_t k = 0; k < reps.size(); ++k) {
+        Replica *r = reps[k];
+        long const most = static_cast<long>(r->n_blocks) * tpa;
+        long nb = (static_cast<long>(kTargetBlocks) * r->n_blocks + total - 1) / total;
+        nb = std::max(1L, std::min(nb, most));
+        if (density) {
+            r->dblk_begin = static_cast<int>(blk_rep.size());
+            r->dblk_n = static_cast<int>(nb);
+        } else {
+            r->fblk_begin = static_cast<int>(blk_rep.size());
+            r->fblk_n = static_cast<int>(nb);
+        }
+        blk_rep.insert(blk_rep.end(), static_cast<size_t>(nb), static_cast<int>(k));
+    }
+    return static_cast<int>(blk_rep.size());
+}
+
+char const *fatal_message(unsigned bits) {
+    if (bits & MDELAST_FATAL_RHO_MAX)
+        return "FATAL: EAM F rho >rhomax_fatal";
+    if (bits & MDELAST_FATAL_VOLUME)
+        return "FATAL: volume change too large...";
+    if (bits & MDELAST_FATAL_MOMENTUM)
+        return "FATAL: total momentum";
+    if (bits & MDELAST_FATAL_PRESSURE)
+        return "FATAL PRESS";
+    if (bits & MDELAST_FATAL_CONSERVATION)
+        return "FATAL: bad energy conservation...";
+    if (bits & MDELAST_ERR_LIST_OVERFLOW)
+        return "neighbour list capacity exceeded";
+    if (bits & MDELAST_ERR_CELL_OVERFLOW)
+        return "cell list capacity exceeded";
+    return "FATAL";
+}
+
+} // namespace
+
+struct mdelast_driver_s {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int N = 0, n_pad = 0, n_rep = 1, ntypes = 0, npot = 0, n_blocks = 0;
+    int tpa_d = 1, tpa_f = 1; // lanes per atom of the density and force passes
+    int grid_d = 1, grid_f = 1; // blocks of the density and force passes
+    int *d_dblk_rep = nullptr, *d_fblk_rep = nullptr;
+    int neighbors = 0;
+    double r_skin = 1., r_list = 0.;
+    int sample = 1;
+    bool stepped = false, obs_valid = false, dead = false;
+    unsigned dead_bits = 0;
+
+    Replica *d_rep = nullptr;
+    int *d_rep_of = nullptr;
+    double4 *d_crd = nullptr;
+    double *d_vel = nullptr, *d_frc = nullptr, *d_rho = nullptr, *d_Fe = nullptr,
+           *d_epot = nullptr;
+    double2 *d_dF2 = nullptr;
+    int *d_nbr = nullptr, *d_nup = nullptr, *d_ndn = nullptr;
+    double *d_pd = nullptr, *d_pf = nullptr;
+    int *d_cell_count = nullptr, *d_cell_atoms = nullptr, *d_max_count = nullptr;
+    double *d_rb = nullptr, *d_Ft = nullptr;
+    double *d_pos0 = nullptr, *d_out = nullptr;
+    int *d_tmp_i = nullptr;
+    size_t tmp_i_cap = 0;
+
+    AtomsView A{};
+    TablesView T{};
+    mdelast_observables *h_obs = nullptr; // pinned, n_rep entries
+    cudaEvent_t ev_step = nullptr;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    bool all_pairs = false; // every replica lists by all-pairs search
+
+    ~mdelast_driver_s();
+    int alloc_list(int maxn);
+    int alloc_cells(int n_cells, int cell_cap);
+    void drop_graphs();
+    int cells_alloc = 0;
+    int configure_cells(double const h[3]);
+    int enqueue_rebuild();
+    int build_list_checked();
+    int enqueue_step(int obs);
+    int wait_step();
+    int check_status();
+};
+
+mdelast_driver_s::~mdelast_driver_s() {
+    if (device >= 0)
+        cudaSetDevice(device);
+    for (auto &g : graph)
+        if (g)
+            cudaGraphExecDestroy(g);
+    if (ev_step)
+        cudaEventDestroy(ev_step);
+    if (h_obs)
+        cudaFreeHost(h_obs);
+    dfree(d_rep);
+    dfree(d_rep_of);
+    dfree(d_crd);
+    dfree(d_vel);
+    dfree(d_frc);
+    dfree(d_rho);
+    dfree(d_Fe);
+    dfree(d_epot);
+    dfree(d_dF2);
+    dfree(d_nbr);
+    dfree(d_nup);
+    dfree(d_ndn);
+    dfree(d_pd);
+    dfree(d_pf);
+    dfree(d_cell_count);
+    dfree(d_cell_atoms);
+    dfree(d_max_count);
+    dfree(d_rb);
+    dfree(d_Ft);
+    dfree(d_pos0);
+    dfree(d_out);
+    dfree(d_tmp_i);
+    dfree(d_dblk_rep);
+    dfree(d_fblk_rep);
+    if (stream)
+        cudaStreamDestroy(stream);
+}
+
+int mdelast_driver_s::alloc_list(int maxn) {
+    dfree(d_nbr);
+    if (int rc = dalloc(&d_nbr, static_cast<size_t>(maxn) * n_pad))
+        return rc;
+    A.nbr = d_nbr;
+    A.maxn = maxn;
+    drop_graphs();
+    return MDELAST_OK;
+}
+
+int mdelast_driver_s::alloc_cells(int n_cells, int cell_cap) {
+    dfree(d_cell_count);
+    dfree(d_cell_atoms);
+    if (int rc = dalloc(&d_cell_count, static_cast<size_t>(std::max(n_cells, 1))))
+        return rc;
+    if (int rc = dalloc(&d_cell_atoms, static_cast<size_t>(std::max(n_cells, 1)) * cell_cap))
+        return rc;
+    A.cell_count = d_cell_count;
+    A.cell_atoms = d_cell_atoms;
+    cells_alloc = n_cells;
+    A.cell_cap = cell_cap;
+    drop_graphs();
+    return MDELAST_OK;
+}
+
+void mdelast_driver_s::drop_graphs() {
+    for (auto &g : graph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+}
+
+// Cells per edge for the current box: no cell thinner than the list radius (with a margin
+// for the box changes of an NPT run between rebuilds); fewer than 3 along any edge means
+// an all-pairs search.
+int mdelast_driver_s::configure_cells(double const h[3]) {
+    int nc[3];
+    bool brute = false;
+    for (int a = 0; a < 3; ++a) {
+        nc[a] = static_cast<int>(std::floor(h[a] / (r_list * 1.05)));
+        if (nc[a] < 3)
+            brute = true;
+    }
+    if (brute)
+        nc[0] = nc[1] = nc[2] = 0;
+    int const n_cells = brute ? 0 : nc[0] * nc[1] * nc[2];
+    Replica r;
+    CK(cudaMemcpy(&r, d_rep, sizeof(Replica), cudaMemcpyDeviceToHost));
+    bool const changed = r.nc[0] != nc[0] || r.nc[1] != nc[1] || r.nc[2] != nc[2];
+    if (changed) {
+        r.nc[0] = nc[0];
+        r.nc[1] = nc[1];
+        r.nc[2] = nc[2];
+        r.cell_begin = 0;
+        CK(cudaMemcpy(d_rep, &r, sizeof(Replica), cudaMemcpyHostToDevice));
+    }
+    int cap = std::max(A.cell_cap, 64);
+    if (n_cells > 0)
+        cap = std::max(cap, static_cast<int>(2. * N / n_cells) + 64);
+    if (!d_cell_count || n_cells > cells_alloc || cap > A.cell_cap)
+        if (int rc = alloc_cells(std::max(n_cells, cells_alloc), cap))
+            return rc;
+    if (changed || all_pairs != brute || A.n_cells != n_cells)
+        drop_graphs(); // the launch shape of the cell kernels is part of the graphs
+    all_pairs = brute;
+    A.n_cells = n_cells;
+    return MDELAST_OK;
+}
+
+int mdelast_driver_s::enqueue_rebuild() {
+    CK(cudaMemsetAsync(d_max_count, 0, 2 * sizeof(int), stream));
+    int const grid = n_pad / kBlock;
+    if (!all_pairs && A.n_cells > 0) {
+        CK(cudaMemsetAsync(d_cell_count, 0, sizeof(int) * A.n_cells, stream));
+        k_cell_bin<<<grid, kBlock, 0, stream>>>(A);
+        k_cell_sort<<<A.n_cells, 128, sizeof(int) * A.cell_cap, stream>>>(A);
+    }
+    k_nbr_build<<<n_pad / 8, 256, 0, stream>>>(A); // one warp per atom slot
+    CK(cudaGetLastError());
+    return MDELAST_OK;
+}
+
+// Build the list now and grow the neighbour or cell capacity until it fits.
+int mdelast_driver_s::build_list_checked() {
+    for (int attempt = 0; attempt < 6; ++attempt) {
+        if (int rc = enqueue_rebuild())
+            return rc;
+        int mc[2];
+        CK(cudaMemcpyAsync(mc, d_max_count, sizeof(mc), cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        bool grow = false;
+        if (mc[1] > A.cell_cap) {
+            if (int rc = alloc_cells(cells_alloc, mc[1] + mc[1] / 2 + 32))
+                return rc;
+            grow = true;
+        }
+        if (mc[0] > A.maxn) {
+            int const m = ((mc[0] + mc[0] / 2 + 32) + 3) / 4 * 4;
+            if (int rc = alloc_list(m))
+                return rc;
+            grow = true;
+        }
+        if (!grow)
+            return MDELAST_OK;
+        // the overflow bits of the attempt that did not fit
+        k_status_and<<<1, 32, 0, stream>>>(A, ~(MDELAST_ERR_LIST_OVERFLOW | MDELAST_ERR_CELL_OVERFLOW));
+        CK(cudaGetLastError());
+    }
+    return fail(MDELAST_ERR_CAPACITY, "neighbour list did not fit after repeated growth");
+}
+
+int mdelast_driver_s::enqueue_step(int obs) {
+    int const grid = n_pad / kBlock;
+    k_pre<<<n_rep, 64, 0, stream>>>(A);
+    k_kick_drift<<<grid, kBlock, 0, stream>>>(A, T);
+    if (!neighbors)
+        if (int rc = enqueue_rebuild())
+            return rc;
+    launch_density(obs != 0, tpa_d, grid_d, stream, A, T);
+    launch_force(obs != 0, true, tpa_f, grid_f, stream, A, T);
+    k_post<<<n_rep, 256, 0, stream>>>(A, POST_STEP, obs);
+    CK(cudaGetLastError());
+    CK(cudaMemcpy2DAsync(h_obs, sizeof(mdelast_observables),
+                         reinterpret_cast<char *>(d_rep) + offsetof(Replica, obs), sizeof(Replica),
+                         sizeof(mdelast_observables), n_rep, cudaMemcpyDeviceToHost, stream));
+    return MDELAST_OK;
+}
+
+int mdelast_driver_s::wait_step() {
+    if (!obs_valid) {
+        CK(cudaEventSynchronize(ev_step));
+        obs_valid = true;
+    }
+    return check_status();
+}
+
+int mdelast_driver_s::check_status() {
+    if (dead)
+        return fail(MDELAST_ERR_FATAL, "%s (status 0x%x)", fatal_message(dead_bits), dead_bits);
+    for (int r = 0; r < n_rep; ++r) {
+        unsigned const st = h_obs[r].status;
+        if (st & MDELAST_FATAL_MASK) {
+            dead = true;
+            dead_bits = st;
+            return fail(MDELAST_ERR_FATAL, "%s (status 0x%x)", fatal_message(st), st);
+        }
+    }
+    return MDELAST_OK;
+}
+
+extern "C" {
+
+int mdelast_device_available(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n > 0;
+}
+
+int mdelast_driver_create(const mdelast_driver_config *cfg, mdelast_driver **out) {
+    clear_error();
+    if (!cfg || !out)
+        return fail(MDELAST_ERR_ARGUMENT, "null argument");
+    *out = nullptr;
+    mdelast_driver_config const &c = *cfg;
+    int const N = c.n_atoms, nt = c.n_types;
+    if (N < 2 || nt < 1 || nt > kMaxTypes)
+        return fail(MDELAST_ERR_ARGUMENT, "need n_atoms >= 2 and 1 <= n_types <= %d", kMaxTypes);
+    if (!c.positions || !c.velocities || !c.types || !c.mass || !c.pair)
+        return fail(MDELAST_ERR_ARGUMENT, "null array in the driver configuration");
+    int const npot = nt * (nt + 1) / 2;
+    if (c.n_eam != 0 && c.n_eam != nt)
+        return fail(MDELAST_ERR_ARGUMENT, "EAM objects: %d given, %d types", c.n_eam, nt);
+    if (c.ensemble < MDELAST_NVE || c.ensemble > MDELAST_NPT)
+        return fail(MDELAST_ERR_UNSUPPORTED, "bad ensamble %d", c.ensemble);
+    if (c.coupling < 0 || c.coupling > 2)
+        return fail(MDELAST_ERR_ARGUMENT, "bad thermostat coupling %d", c.coupling);
+    if (!(c.dt > 0.) || !(c.r_skin >= 1.))
+        return fail(MDELAST_ERR_ARGUMENT, "need dt > 0 and r_skin >= 1");
+    if (c.thermo_nchain < 1 || c.thermo_nchain > kMaxChain || c.baro_nchain < 1 ||
+        c.baro_nchain > kMaxChain || !c.thermo_q || !c.thermo_p_eta || !c.baro_q ||
+        !c.baro_p_eta)
+        return fail(MDELAST_ERR_ARGUMENT, "thermostat chains need 1..%d links", kMaxChain);
+    if (c.n_rg < 2 || !c.rg)
+        return fail(MDELAST_ERR_ARGUMENT, "rg needs at least 2 bins");
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b)
+            if (a != b && c.box[3 * a + b] != 0.)
+                return fail(MDELAST_ERR_ARGUMENT, "the box must be diagonal");
+    if (c.precision != MDELAST_PRECISION_FP64)
+        return fail(MDELAST_ERR_UNSUPPORTED, "precision %d is not available", c.precision);
+    // tables: every pair slot and EAM function on one r grid
+    mdelast_pair const *p0 = c.pair[0];
+    for (int s = 0; s < npot; ++s) {
+        mdelast_pair const *p = c.pair[s];
+        if (!p)
+            return fail(MDELAST_ERR_ARGUMENT, "pair slot %d is null", s);
+        if (p->kind != PAIR_TABLE)
+            return fail(MDELAST_ERR_UNSUPPORTED,
+                        "analytic pair potentials (Morse, LennardJones) are not available on "
+                        "the GPU path; tabulate them as TablePotential");
+        if (p->table.n != p0->table.n || p->table.h != p0->table.h)
+            return fail(MDELAST_ERR_UNSUPPORTED, "pair tables on different grids");
+    }
+    for (int t = 0; t < c.n_eam; ++t) {
+        mdelast_eam const *e = c.eam[t];
+        if (!e)
+            return fail(MDELAST_ERR_ARGUMENT, "EAM %d is null", t);
+        if (e->rho.n != p0->table.n || e->rho.h != p0->table.h ||
+            e->F.n != c.eam[0]->F.n || e->F.h != c.eam[0]->F.h)
+            return fail(MDELAST_ERR_UNSUPPORTED, "EAM tables on different grids");
+    }
+    double const L[3] = {c.box[0], c.box[4], c.box[8]};
+    std::vector<double4> crd(static_cast<size_t>(N));
+    for (int i = 0; i < N; ++i) {
+        double const *p = c.positions + 3 * i;
+        // md_driver.cpp:91-106
+        if (std::abs(p[0]) >= 0.5 * L[0] || std::abs(p[1]) >= 0.5 * L[1] ||
+            std::abs(p[2]) >= 0.5 * L[2])
+            return fail(MDELAST_ERR_ARGUMENT, "bad initial position (atom %d)", i);
+        if (c.types[i] >= static_cast<uint32_t>(nt))
+            return fail(MDELAST_ERR_ARGUMENT, "bad type (atom %d)", i);
+        double u[3] = {p[0] / L[0], p[1] / L[1], p[2] / L[2]};
+        crd[i] = make_double4(u[0] - nint_host(u[0]), u[1] - nint_host(u[1]),
+                              u[2] - nint_host(u[2]), static_cast<double>(c.types[i]));
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(MDELAST_ERR_NO_DEVICE, "no CUDA device: the mdelast GPU path needs one");
+    }
+    if (c.device < 0 || c.device >= ndev)
+        return fail(MDELAST_ERR_ARGUMENT, "device %d not present (%d devices)", c.device, ndev);
+    CK(cudaSetDevice(c.device));
+
+    auto *d = new mdelast_driver_s();
+    d->device = c.device;
+    auto bail = [&](int rc) {
+        delete d;
+        return rc;
+    };
+#define TRY(x)                                                                                \
+    do {                                                                                      \
+        int rc_ = (x);                                                                        \
+        if (rc_)                                                                              \
+            return bail(rc_);                                                                 \
+    } while (0)
+    if (cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(fail(MDELAST_ERR_CUDA, "stream creation failed"));
+    d->N = N;
+    d->ntypes = nt;
+    d->npot = npot;
+    d->n_pad = (N + kTile - 1) / kTile * kTile;
+    d->n_blocks = d->n_pad / kBlock;
+    d->neighbors = c.neighbors != 0;
+    d->r_skin = c.r_skin;
+    double const rcut = p0->rcut;
+    d->r_list = d->neighbors ? rcut * c.r_skin : rcut;
+    int const np = d->n_pad;
+
+    // ---- tables: r-table bundles and embedding tables
+    int const nri = p0->table.n;
+    std::vector<double> rb(static_cast<size_t>(npot) * nri * 18, 0.);
+    for (int b = 0; b < nt; ++b)
+        for (int a = 0; a <= b; ++a) {
+            int const s = b * (b + 1) / 2 + a;
+            for (int k = 0; k < nri; ++k) {
+                double *o = rb.data() + (static_cast<size_t>(s) * nri + k) * 18;
+                std::memcpy(o, c.pair[s]->table.coef.data() + 6 * static_cast<size_t>(k),
+                            6 * sizeof(double));
+                if (c.n_eam) {
+                    std::memcpy(o + 6, c.eam[a]->rho.coef.data() + 6 * static_cast<size_t>(k),
+                                6 * sizeof(double));
+                    std::memcpy(o + 12, c.eam[b]->rho.coef.data() + 6 * static_cast<size_t>(k),
+                                6 * sizeof(double));
+                }
+            }
+        }
+    int const nfi = c.n_eam ? c.eam[0]->F.n : 1;
+    std::vector<double> Ft(static_cast<size_t>(nt) * nfi * 6, 0.);
+    for (int t = 0; t < c.n_eam; ++t)
+        std::memcpy(Ft.data() + static_cast<size_t>(t) * nfi * 6, c.eam[t]->F.coef.data(),
+                    sizeof(double) * 6 * nfi);
+    TRY(dalloc(&d->d_rb, rb.size()));
+    TRY(dalloc(&d->d_Ft, Ft.size()));
+    if (cudaMemcpy(d->d_rb, rb.data(), sizeof(double) * rb.size(), cudaMemcpyHostToDevice) ||
+        cudaMemcpy(d->d_Ft, Ft.data(), sizeof(double) * Ft.size(), cudaMemcpyHostToDevice))
+        return bail(fail(MDELAST_ERR_CUDA, "table upload failed"));
+    TablesView &T = d->T;
+    T.rb = d->d_rb;
+    T.nri = nri;
+    T.npot = npot;
+    T.inv_hr = p0->table.inv_h;
+    T.inv_hr2 = p0->table.inv_h2;
+    T.Ft = d->d_Ft;
+    T.nfi = nfi;
+    T.ntypes = nt;
+    T.inv_hf = c.n_eam ? c.eam[0]->F.inv_h : 1.;
+    T.inv_hf2 = c.n_eam ? c.eam[0]->F.inv_h2 : 1.;
+    T.has_eam = c.n_eam > 0;
+    T.r_cut_sq = rcut * rcut;
+    for (int s = 0; s < npot; ++s) {
+        T.pot_rcut[s] = c.pair[s]->rcut;
+        T.pot_rmin[s] = c.pair[s]->rmin_fatal;
+    }
+    for (int t = 0; t < nt; ++t) {
+        T.eam_rcut[t] = c.n_eam ? c.eam[t]->rcut : 0.;
+        T.rhomax[t] = c.n_eam ? c.eam[t]->rhomax_fatal : 0.;
+        T.mass[t] = c.mass[t];
+    }
+
+    // ---- replica state
+    Replica R;
+    std::memset(&R, 0, sizeof(R));
+    R.atom_begin = 0;
+    R.n_atoms = N;
+    R.block_begin = 0;
+    R.n_blocks = d->n_blocks;
+    R.ensemble = c.ensemble;
+    R.coupling = c.coupling;
+    R.Nf = c.Nf;
+    R.alpha = 1. + 3. / c.Nf;
+    R.dt = c.dt;
+    R.fatal_conservation = c.fatal_conservation;
+    R.mass0 = c.mass[0];
+    R.baro_P = c.baro_P;
+    R.baro_w = c.baro_w;
+    for (int a = 0; a < 3; ++a)
+        R.h0[a] = R.h[a] = R.h_pos[a] = L[a];
+    R.eps = 0.;
+    R.p_eps = c.baro_p_eps;
+    R.vscale = 1.;
+    auto set_chain = [](Chain &ch, double T_, int n, const double *q, const double *p,
+                        double Nf) {
+        ch.T = T_;
+        ch.Nf = Nf;
+        ch.n = n;
+        for (int j = 0; j < n; ++j) {
+            ch.q[j] = q[j];
+            ch.inv_q[j] = 1. / q[j];
+            ch.p_eta[j] = p[j];
+            ch.eta[j] = 0.;
+        }
+    };
+    set_chain(R.th, c.thermo_T, c.thermo_nchain, c.thermo_q, c.thermo_p_eta, c.thermo_Nf);
+    set_chain(R.bth, c.baro_thermo_T, c.baro_nchain, c.baro_q, c.baro_p_eta, c.baro_Nf);
+
+    d->tpa_d = d->tpa_f = default_tpa(N);
+    std::vector<Replica *> reps{&R};
+    std::vector<int> dmap, fmap;
+    d->grid_d = deal_blocks(reps, d->tpa_d, true, dmap);
+    d->grid_f = deal_blocks(reps, d->tpa_f, false, fmap);
+    TRY(dalloc(&d->d_dblk_rep, dmap.size()));
+    TRY(dalloc(&d->d_fblk_rep, fmap.size()));
+    TRY(dalloc(&d->d_rep, 1));
+    if (cudaMemcpy(d->d_rep, &R, sizeof(R), cudaMemcpyHostToDevice) ||
+        cudaMemcpy(d->d_dblk_rep, dmap.data(), sizeof(int) * dmap.size(), cudaMemcpyHostToDevice) ||
+        cudaMemcpy(d->d_fblk_rep, fmap.data(), sizeof(int) * fmap.size(), cudaMemcpyHostToDevice))
+        return bail(fail(MDELAST_ERR_CUDA, "state upload failed"));
+
+    // ---- atoms
+    std::vector<int> rep_of(static_cast<size_t>(np), -1);
+    std::fill(rep_of.begin(), rep_of.begin() + N, 0);
+    std::vector<double4> crd_pad(static_cast<size_t>(np), make_double4(0, 0, 0, 0));
+    std::copy(crd.begin(), crd.end(), crd_pad.begin());
+    std::vector<double> vel(3 * static_cast<size_t>(np), 0.);
+    for (int i = 0; i < N; ++i)
+        for (int a = 0; a < 3; ++a)
+            vel[static_cast<size_t>(a) * np + i] = c.velocities[3 * i + a];
+    TRY(dalloc(&d->d_rep_of, np));
+    TRY(dalloc(&d->d_crd, np));
+    TRY(dalloc(&d->d_vel, 3 * static_cast<size_t>(np)));
+    TRY(dalloc(&d->d_frc, 3 * static_cast<size_t>(np)));
+    TRY(dalloc(&d->d_rho, np));
+    TRY(dalloc(&d->d_Fe, np));
+    TRY(dalloc(&d->d_epot, np));
+    TRY(dalloc(&d->d_dF2, np));
+    TRY(dalloc(&d->d_nup, np));
+    TRY(dalloc(&d->d_ndn, np));
+    TRY(dalloc(&d->d_pd, static_cast<size_t>(d->grid_d) * D_NSUM));
+    TRY(dalloc(&d->d_pf, static_cast<size_t>(d->grid_f) * F_NSUM));
+    TRY(dalloc(&d->d_max_count, 2));
+    TRY(dalloc(&d->d_pos0, 3 * static_cast<size_t>(N)));
+    TRY(dalloc(&d->d_out, 3 * static_cast<size_t>(N)));
+    if (cudaMemcpy(d->d_rep_of, rep_of.data(), sizeof(int) * np, cudaMemcpyHostToDevice) ||
+        cudaMemcpy(d->d_crd, crd_pad.data(), sizeof(double4) * np, cudaMemcpyHostToDevice) ||
+        cudaMemcpy(d->d_vel, vel.data(), sizeof(double) * vel.size(), cudaMemcpyHostToDevice) ||
+        cudaMemcpy(d->d_pos0, c.positions, sizeof(double) * 3 * N, cudaMemcpyHostToDevice))
+        return bail(fail(MDELAST_ERR_CUDA, "atom upload failed"));
+    if (cudaMallocHost(&d->h_obs, sizeof(mdelast_observables) * d->n_rep) ||
+        cudaEventCreateWithFlags(&d->ev_step, cudaEventDisableTiming))
+        return bail(fail(MDELAST_ERR_CUDA, "host staging allocation failed"));
+
+    AtomsView &A = d->A;
+    A.n_pad = np;
+    A.n_rep = d->n_rep;
+    A.rep = d->d_rep;
+    A.rep_of = d->d_rep_of;
+    A.crd = d->d_crd;
+    A.vel = d->d_vel;
+    A.frc = d->d_frc;
+    A.rho = d->d_rho;
+    A.Fe = d->d_Fe;
+    A.epot = d->d_epot;
+    A.dF2 = d->d_dF2;
+    A.n_up = d->d_nup;
+    A.n_dn = d->d_ndn;
+    A.pd = d->d_pd;
+    A.pf = d->d_pf;
+    A.dblk_rep = d->d_dblk_rep;
+    A.fblk_rep = d->d_fblk_rep;
+    A.max_count = d->d_max_count;
+    A.r_list_sq = d->r_list * d->r_list;
+    if (d->neighbors) // md_driver.cpp:42: pow<2>(pot[0]->rcut * r_skin)
+        A.r_list_sq = (rcut * c.r_skin) * (rcut * c.r_skin);
+    else
+        A.r_list_sq = rcut * rcut;
+
+    // neighbour capacity from the number density: 1.5 x the mean count + 32
+    double const vol = L[0] * (L[1] * L[2]);
+    double const mean = 4. / 3. * M_PI * std::pow(d->r_list, 3) * N / vol;
+    int maxn = static_cast<int>(1.5 * std::min(mean, static_cast<double>(N))) + 32;
+    maxn = std::min((maxn + 3) / 4 * 4, (N + 3) / 4 * 4);
+    TRY(d->alloc_list(std::max(maxn, 4)));
+    TRY(d->configure_cells(L));
+
+    // ---- the constructor's force call and thermodynamics (md_driver.cpp:112-118)
+    TRY(d->build_list_checked());
+    launch_density(true, d->tpa_d, d->grid_d, d->stream, d->A, d->T);
+    launch_force(true, false, d->tpa_f, d->grid_f, d->stream, d->A, d->T);
+    k_post<<<d->n_rep, 256, 0, d->stream>>>(d->A, POST_INIT, 1);
+    if (cudaGetLastError() != cudaSuccess)
+        return bail(fail(MDELAST_ERR_CUDA, "kernel launch failed"));
+    if (cudaMemcpy2DAsync(d->h_obs, sizeof(mdelast_observables),
+                          reinterpret_cast<char *>(d->d_rep) + offsetof(Replica, obs),
+                          sizeof(Replica), sizeof(mdelast_observables), d->n_rep,
+                          cudaMemcpyDeviceToHost, d->stream) ||
+        cudaStreamSynchronize(d->stream))
+        return bail(fail(MDELAST_ERR_CUDA, "constructor force call failed: %s",
+                         cudaGetErrorString(cudaGetLastError())));
+    d->obs_valid = true;
+    TRY(d->check_status());
+#undef TRY
+    *out = d;
+    return MDELAST_OK;
+}
+
+void mdelast_driver_destroy(mdelast_driver *d) { delete d; }
+
+int mdelast_driver_integrate(mdelast_driver *d, int32_t n_steps) {
+    clear_error();
+    if (!d || n_steps < 0)
+        return fail(MDELAST_ERR_ARGUMENT, "bad argument");
+    if (d->dead)
+        return d->check_status();
+    CK(cudaSetDevice(d->device));
+    int const obs = d->sample ? 1 : 0;
+    if (!d->graph[obs]) {
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(d->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = d->enqueue_step(obs);
+        cudaError_t e = cudaStreamEndCapture(d->stream, &g);
+        if (rc)
+            return rc;
+        if (e != cudaSuccess)
+            return fail(MDELAST_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&d->graph[obs], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess)
+            return fail(MDELAST_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    }
+    for (int s = 0; s < n_steps; ++s)
+        CK(cudaGraphLaunch(d->graph[obs], d->stream));
+    if (n_steps > 0) {
+        CK(cudaEventRecord(d->ev_step, d->stream));
+        d->obs_valid = false;
+        d->stepped = true;
+    }
+    return MDELAST_OK;
+}
+
+int mdelast_driver_calculate_neighbors(mdelast_driver *d) {
+    clear_error();
+    if (!d)
+        return fail(MDELAST_ERR_ARGUMENT, "null driver");
+    CK(cudaSetDevice(d->device));
+    if (int rc = d->wait_step())
+        return rc;
+    if (!d->neighbors) // the reference writes into empty point/neighbors storage
+        return fail(MDELAST_ERR_UNSUPPORTED,
+                    "calculate_neighbors() needs a driver created with neighbors=True");
+    double h[3] = {d->h_obs[0].box[0], d->h_obs[0].box[4], d->h_obs[0].box[8]};
+    if (int rc = d->configure_cells(h))
+        return rc;
+    return d->build_list_checked();
+}
+
+int mdelast_driver_set_sample_observables(mdelast_driver *d, int32_t flag) {
+    if (!d)
+        return fail(MDELAST_ERR_ARGUMENT, "null driver");
+    d->sample = flag != 0;
+    return MDELAST_OK;
+}
+
+int mdelast_driver_get_sample_observables(const mdelast_driver *d, int32_t *flag) {
+    if (!d || !flag)
+        return fail(MDELAST_ERR_ARGUMENT, "null argument");
+    *flag = d->sample;
+    return MDELAST_OK;
+}
+
+int mdelast_driver_synchronize(mdelast_driver *d) {
+    clear_error();
+    if (!d)
+        return fail(MDELAST_ERR_ARGUMENT, "null driver");
+    CK(cudaSetDevice(d->device));
+    CK(cudaStreamSynchronize(d->stream));
+    return d->wait_step();
+}
+
+int mdelast_driver_get_observables(mdelast_driver *d, mdelast_observables *out) {
+    clear_error();
+    if (!d || !out)
+        return fail(MDELAST_ERR_ARGUMENT, "null argument");
+    CK(cudaSetDevice(d->device));
+    int const rc = d->wait_step();
+    *out = d->h_obs[0];
+    return rc;
+}
+
+int mdelast_driver_get_atoms(mdelast_driver *d, int32_t field, double *out) {
+    clear_error();
+    if (!d || !out || field < 0 || field > MDELAST_ATOM_EKIN)
+        return fail(MDELAST_ERR_ARGUMENT, "bad argument");
+    CK(cudaSetDevice(d->device));
+    if (int rc = d->wait_step())
+        return rc;
+    int const N = d->N;
+    k_readout<<<(N + 255) / 256, 256, 0, d->stream>>>(d->A, d->T, 0, field, d->d_out, d->d_pos0,
+                                                      d->stepped ? 1 : 0);
+    CK(cudaGetLastError());
+    size_t const n = field <= MDELAST_ATOM_FORCES ? 3 * static_cast<size_t>(N) : N;
+    CK(cudaMemcpyAsync(out, d->d_out, sizeof(double) * n, cudaMemcpyDeviceToHost, d->stream));
+    CK(cudaStreamSynchronize(d->stream));
+    return MDELAST_OK;
+}
+
+int mdelast_driver_get_chain(mdelast_driver *d, int32_t which, double *q, double *p_eta,
+                             double *eta, int32_t *nchain) {
+    clear_error();
+    if (!d || (which != 0 && which != 1))
+        return fail(MDELAST_ERR_ARGUMENT, "bad argument");
+    CK(cudaSetDevice(d->device));
+    if (int rc = d->wait_step())
+        return rc;
+    Chain ch;
+    size_t const off = which == 0 ? offsetof(Replica, th) : offsetof(Replica, bth);
+    CK(cudaMemcpy(&ch, reinterpret_cast<char *>(d->d_rep) + off, sizeof(Chain),
+                  cudaMemcpyDeviceToHost));
+    for (int j = 0; j < ch.n; ++j) {
+        if (q)
+            q[j] = ch.q[j];
+        if (p_eta)
+            p_eta[j] = ch.p_eta[j];
+        if (eta)
+            eta[j] = ch.eta[j];
+    }
+    if (nchain)
+        *nchain = ch.n;
+    return MDELAST_OK;
+}
+
+int mdelast_driver_get_neighbors(mdelast_driver *d, int32_t *point, int32_t *neighbors,
+                                 int64_t cap, int64_t *n_entries) {
+    clear_error();
+    if (!d || !point)
+        return fail(MDELAST_ERR_ARGUMENT, "null argument");
+    if (!d->neighbors)
+        return fail(MDELAST_ERR_UNSUPPORTED, "neighbour lists are disabled for this driver");
+    CK(cudaSetDevice(d->device));
+    if (int rc = d->wait_step())
+        return rc;
+    int const N = d->N;
+    if (d->tmp_i_cap < static_cast<size_t>(N) + 1) {
+        dfree(d->d_tmp_i);
+        if (int rc = dalloc(&d->d_tmp_i, static_cast<size_t>(N) + 1))
+            return rc;
+        d->tmp_i_cap = static_cast<size_t>(N) + 1;
+    }
+    k_half_list_counts<<<(N + 255) / 256, 256, 0, d->stream>>>(d->A, 0, d->d_tmp_i);
+    std::vector<int> cnt(static_cast<size_t>(N));
+    CK(cudaMemcpyAsync(cnt.data(), d->d_tmp_i, sizeof(int) * N, cudaMemcpyDeviceToHost,
+                       d->stream));
+    CK(cudaStreamSynchronize(d->stream));
+    int64_t total = 0;
+    for (int i = 0; i < N; ++i) {
+        point[i] = static_cast<int32_t>(total);
+        total += cnt[static_cast<size_t>(i)];
+    }
+    point[N] = static_cast<int32_t>(total);
+    if (n_entries)
+        *n_entries = total;
+    if (!neighbors || cap <= 0)
+        return MDELAST_OK;
+    int *d_point = nullptr, *d_list = nullptr;
+    if (int rc = dalloc(&d_point, static_cast<size_t>(N) + 1))
+        return rc;
+    if (int rc = dalloc(&d_list, static_cast<size_t>(std::max<int64_t>(total, 1)))) {
+        dfree(d_point);
+        return rc;
+    }
+    cudaMemcpy(d_point, point, sizeof(int) * (N + 1), cudaMemcpyHostToDevice);
+    k_half_list_fill<<<(N + 255) / 256, 256, 0, d->stream>>>(d->A, 0, d_point, d_list);
+    cudaError_t e = cudaMemcpyAsync(neighbors, d_list,
+                                    sizeof(int) * static_cast<size_t>(std::min(total, cap)),
+                                    cudaMemcpyDeviceToHost, d->stream);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(d->stream);
+    dfree(d_point);
+    dfree(d_list);
+    if (e != cudaSuccess)
+        return fail(MDELAST_ERR_CUDA, "neighbour readout: %s", cudaGetErrorString(e));
+    return MDELAST_OK;
+}
+
+int mdelast_driver_pair_correlation(mdelast_driver *d, int32_t mode) {
+    (void)d;
+    (void)mode;
+    return fail(MDELAST_ERR_UNSUPPORTED, "pair correlation is not available yet");
+}
+
+int mdelast_driver_get_gr(mdelast_driver *d, double *gr, double *gr_partial) {
+    (void)d;
+    (void)gr;
+    (void)gr_partial;
+    return fail(MDELAST_ERR_UNSUPPORTED, "pair correlation is not available yet");
+}
+
+int mdelast_table_eval_device(const mdelast_pair *p, const mdelast_eam *e, int which,
+                              const double *x, int64_t n, double *out) {
+    clear_error();
+    if (!x || !out || n < 0 || which < 0 || which > 2 || (which == 0 && !p) ||
+        (which > 0 && !e))
+        return fail(MDELAST_ERR_ARGUMENT, "bad argument");
+    if (which == 0 && p->kind != PAIR_TABLE)
+        return fail(MDELAST_ERR_UNSUPPORTED, "analytic pair potentials have no device table");
+    if (!mdelast_device_available())
+        return fail(MDELAST_ERR_NO_DEVICE, "no CUDA device");
+    // a one-type table set holding just this function
+    mdelast::QuinticTable const &tab = which == 0 ? p->table : (which == 1 ? e->rho : e->F);
+    int const nint = tab.n;
+    std::vector<double> rb, Ft;
+    TablesView T{};
+    if (which == 2) {
+        Ft.assign(tab.coef.begin(), tab.coef.end());
+        rb.assign(18, 0.);
+        T.nfi = nint;
+        T.inv_hf = tab.inv_h;
+        T.inv_hf2 = tab.inv_h2;
+        T.nri = 1;
+    } else {
+        rb.assign(static_cast<size_t>(nint) * 18, 0.);
+        for (int k = 0; k < nint; ++k)
+            std::memcpy(rb.data() + static_cast<size_t>(k) * 18 + (which == 0 ? 0 : 6),
+                        tab.coef.data() + 6 * static_cast<size_t>(k), 6 * sizeof(double));
+        Ft.assign(6, 0.);
+        T.nri = nint;
+        T.inv_hr = tab.inv_h;
+        T.inv_hr2 = tab.inv_h2;
+        T.nfi = 1;
+    }
+    T.npot = 1;
+    T.ntypes = 1;
+    T.pot_rcut[0] = which == 0 ? p->rcut : 0.;
+    T.eam_rcut[0] = which == 1 ? e->rcut : 0.;
+    double *d_rb = nullptr, *d_Ft = nullptr, *d_x = nullptr, *d_o = nullptr;
+    int rc = MDELAST_OK;
+    if ((rc = dalloc(&d_rb, rb.size())) || (rc = dalloc(&d_Ft, Ft.size())) ||
+        (rc = dalloc(&d_x, static_cast<size_t>(n))) || (rc = dalloc(&d_o, 3 * static_cast<size_t>(n)))) {
+        dfree(d_rb);
+        dfree(d_Ft);
+        dfree(d_x);
+        dfree(d_o);
+        return rc;
+    }
+    T.rb = d_rb;
+    T.Ft = d_Ft;
+    cudaError_t err = cudaMemcpy(d_rb, rb.data(), sizeof(double) * rb.size(), cudaMemcpyHostToDevice);
+    if (!err)
+        err = cudaMemcpy(d_Ft, Ft.data(), sizeof(double) * Ft.size(), cudaMemcpyHostToDevice);
+    if (!err)
+        err = cudaMemcpy(d_x, x, sizeof(double) * n, cudaMemcpyHostToDevice);
+    if (!err && n > 0) {
+        k_table_eval<<<static_cast<unsigned>((n + 255) / 256), 256>>>(T, which, 0, d_x,
+                                                                       static_cast<int>(n), d_o);
+        err = cudaGetLastError();
+    }
+    if (!err)
+        err = cudaMemcpy(out, d_o, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost);
+    dfree(d_rb);
+    dfree(d_Ft);
+    dfree(d_x);
+    dfree(d_o);
+    if (err)
+        return fail(MDELAST_ERR_CUDA, "device table evaluation: %s", cudaGetErrorString(err));
+    return MDELAST_OK;
+}
+
+} // extern "C"

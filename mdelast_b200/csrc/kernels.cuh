@@ -1,0 +1,32 @@
+// Kernel declarations shared by the step orchestration (driver.cu) and the kernel files.
+#pragma once
+
+#include "device.cuh"
+
+namespace mdelast {
+
+// scalar-kernel modes
+enum PostMode : int { POST_INIT = 0, POST_STEP = 1 };
+
+__global__ void k_cell_bin(AtomsView A);
+__global__ void k_cell_sort(AtomsView A);
+__global__ void k_nbr_build(AtomsView A);
+// launchers of the templated pair kernels (defined beside them); tpa = lanes per atom,
+// one of 1, 4, 8, 16 (valid_tpa)
+bool valid_tpa(int tpa);
+void launch_density(bool obs, int tpa, int grid, cudaStream_t s, AtomsView const &A,
+                    TablesView const &T);
+void launch_force(bool obs, bool kick, int tpa, int grid, cudaStream_t s, AtomsView const &A,
+                  TablesView const &T);
+__global__ void k_kick_drift(AtomsView A, TablesView T);
+__global__ void k_pre(AtomsView A);
+__global__ void k_post(AtomsView A, int mode, int obs);
+__global__ void k_readout(AtomsView A, TablesView T, int r, int field, double *out,
+                          const double *pos0, int stepped);
+__global__ void k_half_list_counts(AtomsView A, int r, int *counts);
+__global__ void k_half_list_fill(AtomsView A, int r, const int *point, int *out);
+__global__ void k_status_and(AtomsView A, unsigned mask);
+__global__ void k_table_eval(TablesView T, int which, int s, const double *x, int n,
+                             double *out);
+
+} // namespace mdelast

@@ -1,0 +1,473 @@
+// Per-replica scalar work of a step: the Nose-Hoover-chain thermostat and barostat
+// propagators (thermostat.cpp:40-66, md_driver.cpp:454-561), the coefficients of the
+// kick and drift, the deterministic reduction of the atom kernels' block sums, and the
+// thermodynamics with the reference's fatal checks (md_driver.cpp:603-730).
+//
+// One block per replica. The particle thermostat chain and the barostat chain are
+// independent within a half step and run side by side on the first threads of two warps.
+#include "kernels.cuh"
+
+namespace mdelast {
+
+namespace {
+
+__constant__ double c_wsy7[7] = {
+    0.784513610477560, 0.235573213359357, -1.17767998417887,
+    1. - 2. * (0.784513610477560 + 0.235573213359357 - 1.17767998417887),
+    -1.17767998417887, 0.235573213359357, 0.784513610477560}; // numerics.hpp:22-27
+
+constexpr double kBoltz = 1.38064852e-16; // units.hpp:7
+
+// exp(-x) and op(x) = (1 - exp(-x))/x of numerics.hpp:11-18. For |x| <= 1e-3, op is the
+// reference's own 5th-order Taylor polynomial. For |x| <= 1/16 both functions come from
+// their Taylor series, exp(-x) = sum (-x)^k/k! and op(x) = sum (-x)^k/(k+1)!, to degree 11
+// (the first omitted term is below 1e-23 relative), evaluated by Estrin's scheme: a
+// dependent chain of four FMAs instead of a library exp followed by a division, which
+// matters because the chain sweeps are sequential. For larger |x|, exp() and the
+// division as in the reference. Thermostat arguments are x = dt p_eta/Q ~ dt/tau, so the
+// series branch is the common one.
+__device__ __forceinline__ void expx_operator(double x, double &expx, double &op) {
+    double const ax = fabs(x);
+    if (ax <= 0.0625) {
+        double const y = -x, y2 = y * y, y4 = y2 * y2, y8 = y4 * y4;
+        double const a0 = fma(y, 1.0, 1.0), a1 = fma(y, 1.0 / 6.0, 0.5),
+                     a2 = fma(y, 1.0 / 120.0, 1.0 / 24.0), a3 = fma(y, 1.0 / 5040.0, 1.0 / 720.0),
+                     a4 = fma(y, 1.0 / 362880.0, 1.0 / 40320.0),
+                     a5 = fma(y, 1.0 / 39916800.0, 1.0 / 3628800.0);
+        expx = fma(y8, fma(y2, a5, a4), fma(y4, fma(y2, a3, a2), fma(y2, a1, a0)));
+        if (ax > 1e-3) {
+            double const b0 = fma(y, 0.5, 1.0), b1 = fma(y, 1.0 / 24.0, 1.0 / 6.0),
+                         b2 = fma(y, 1.0 / 720.0, 1.0 / 120.0),
+                         b3 = fma(y, 1.0 / 40320.0, 1.0 / 5040.0),
+                         b4 = fma(y, 1.0 / 3628800.0, 1.0 / 362880.0),
+                         b5 = fma(y, 1.0 / 479001600.0, 1.0 / 39916800.0);
+            op = fma(y8, fma(y2, b5, b4), fma(y4, fma(y2, b3, b2), fma(y2, b1, b0)));
+        } else {
+            double const c1 = -1.0 / 2.0, c2 = 1.0 / 6.0, c3 = -1.0 / 24.0, c4 = 1. / 120.,
+                         c5 = -1. / 720.;
+            op = 1.0 + x * (c1 + x * (c2 + x * (c3 + x * (c4 + x * c5))));
+        }
+        return;
+    }
+    double const e = exp(-x);
+    expx = e;
+    op = (1.0 - e) / x;
+}
+
+__device__ __forceinline__ double volume(const double h[3]) { return h[0] * (h[1] * h[2]); }
+
+// A chain of NC links held in registers while it is propagated: NC is a template
+// parameter (dispatched from the runtime chain length), so the loops unroll exactly and no
+// predicated-off link sits on the sequential critical path of a sweep.
+template <int NC> struct ChainR {
+    double p[NC], iq[NC], eta[NC];
+    double kT, Nf;
+};
+
+template <int NC> __device__ __forceinline__ void chain_load(Chain const &c, ChainR<NC> &r) {
+    r.Nf = c.Nf;
+    r.kT = kBoltz * c.T;
+#pragma unroll
+    for (int j = 0; j < NC; ++j) {
+        r.p[j] = c.p_eta[j];
+        r.iq[j] = c.inv_q[j];
+        r.eta[j] = c.eta[j];
+    }
+}
+
+template <int NC> __device__ __forceinline__ void chain_store(ChainR<NC> const &r, Chain &c) {
+#pragma unroll
+    for (int j = 0; j < NC; ++j) {
+        c.p_eta[j] = r.p[j];
+        c.eta[j] = r.eta[j];
+    }
+}
+
+// thermostat.cpp:40-66 (Yu et al., Chem. Phys. 370 (2010) 294, eq. 8; Allen-Tildesley
+// eqs. 3.73-3.74a): one sweep of the chain. Inward (top link first) each link needs the
+// updated link above it, so its exponential is on the critical path; outward every
+// exponential uses the not-yet-updated link above and all are formed up front.
+template <int NC> __device__ __forceinline__ void U4_in(ChainR<NC> &c, double dt, double ec) {
+#pragma unroll
+    for (int j = NC - 1; j >= 0; --j) {
+        double G;
+        if (j != 0)
+            G = c.p[j - 1] * c.p[j - 1] * c.iq[j - 1] - c.kT;
+        else
+            G = 2. * ec - c.Nf * c.kT;
+        if (j == NC - 1) {
+            c.p[j] += dt * G;
+        } else {
+            double e, op;
+            expx_operator(dt * c.p[j + 1] * c.iq[j + 1], e, op);
+            c.p[j] = c.p[j] * e + dt * G * op;
+        }
+    }
+}
+
+template <int NC> __device__ __forceinline__ void U4_out(ChainR<NC> &c, double dt, double ec) {
+    double e[NC], op[NC];
+#pragma unroll
+    for (int j = 0; j < NC - 1; ++j)
+        expx_operator(dt * c.p[j + 1] * c.iq[j + 1], e[j], op[j]);
+#pragma unroll
+    for (int j = 0; j < NC; ++j) {
+        double G;
+        if (j != 0)
+            G = c.p[j - 1] * c.p[j - 1] * c.iq[j - 1] - c.kT;
+        else
+            G = 2. * ec - c.Nf * c.kT;
+        if (j == NC - 1)
+            c.p[j] += dt * G;
+        else
+            c.p[j] = c.p[j] * e[j] + dt * G * op[j];
+    }
+}
+
+// thermostat.hpp:24-35: factor exp(-dt p_eta[0]/Q[0]) for the coupled momenta; advances
+// the chain positions
+template <int NC> __device__ __forceinline__ double U3(ChainR<NC> &c, double dt) {
+    double s, op;
+    expx_operator(dt * c.p[0] * c.iq[0], s, op);
+#pragma unroll
+    for (int j = 0; j < NC; ++j)
+        c.eta[j] += dt * c.p[j] * c.iq[j];
+    return s;
+}
+
+// thermostat.cpp:24-37
+__device__ double chain_etot(Chain const &c) {
+    double e = c.Nf * c.eta[0];
+    for (int j = 1; j < c.n; ++j)
+        e += c.eta[j];
+    e *= kBoltz * c.T;
+    for (int j = 0; j < c.n; ++j)
+        e += 0.5 * (c.p_eta[j] * c.p_eta[j]) / c.q[j];
+    return e;
+}
+
+// md_driver.cpp:539-549 with U4 coupling of md_driver.cpp:512-531. The velocities are not
+// touched: the product of the seven U3 factors is returned and applied by the next atom
+// kernel; the kinetic energy follows each factor as ekin * s^2.
+template <int NC>
+__device__ double nhc_thermo_n(Chain &gc, double dt, double &ekin, bool conf, bool average,
+                               double econf) {
+    ChainR<NC> c;
+    chain_load<NC>(gc, c);
+    double S = 1.;
+#pragma unroll 1
+    for (int k = 0; k < 7; ++k) {
+        double const dtw = c_wsy7[k] * dt;
+        U4_in<NC>(c, 0.5 * dtw, !conf ? ekin : (average ? 0.5 * (ekin + econf) : econf));
+        double const s = U3<NC>(c, dtw);
+        S *= s;
+        ekin = ekin * s * s;
+        U4_out<NC>(c, 0.5 * dtw, !conf ? ekin : (average ? 0.5 * (ekin + econf) : econf));
+    }
+    chain_store<NC>(c, gc);
+    return S;
+}
+
+// md_driver.cpp:551-561, 533-537, 507-510
+template <int NC> __device__ double nhc_baro_n(Chain &gc, double dt, double p, double iw) {
+    ChainR<NC> c;
+    chain_load<NC>(gc, c);
+#pragma unroll 1
+    for (int k = 0; k < 7; ++k) {
+        double const dtw = c_wsy7[k] * dt;
+        U4_in<NC>(c, 0.5 * dtw, 0.5 * (p * p) * iw);
+        p *= U3<NC>(c, dtw);
+        U4_out<NC>(c, 0.5 * dtw, 0.5 * (p * p) * iw);
+    }
+    chain_store<NC>(c, gc);
+    return p;
+}
+
+#define MDELAST_CHAIN_CASES(F)                                                                \
+    F(1) F(2) F(3) F(4) F(5) F(6) F(7) F(8) F(9) F(10) F(11) F(12) F(13) F(14) F(15) F(16)
+
+__device__ double nhc_thermo(Replica *R, Chain &gc, double dt, double &ekin) {
+    double const tci = R->obs.temperature_conf_inverse;
+    bool const conf = R->coupling != MDELAST_THERMOSTAT_KINETIC && tci != 0.;
+    if (R->coupling != MDELAST_THERMOSTAT_KINETIC && tci == 0.)
+        atomicOr(&R->obs.status, MDELAST_WARN_TCONF_ZERO);
+    double const econf = conf ? (kBoltz / tci) * R->Nf / 2. : 0.;
+    bool const average = R->coupling == MDELAST_THERMOSTAT_AVERAGE;
+    switch (gc.n) {
+#define F(N)                                                                                  \
+    case N:                                                                                   \
+        return nhc_thermo_n<N>(gc, dt, ekin, conf, average, econf);
+        MDELAST_CHAIN_CASES(F)
+#undef F
+    default:
+        return 1.;
+    }
+}
+
+__device__ void nhc_baro(Replica *R, Chain &gc, double dt) {
+    double const iw = 1. / R->baro_w;
+    double p = R->p_eps;
+    switch (gc.n) {
+#define F(N)                                                                                  \
+    case N:                                                                                   \
+        p = nhc_baro_n<N>(gc, dt, p, iw);                                                     \
+        break;
+        MDELAST_CHAIN_CASES(F)
+#undef F
+    default:
+        break;
+    }
+    R->p_eps = p;
+}
+
+// md_driver.cpp:454-459 (Yu et al. eq. 31)
+__device__ void U2p(Replica *R, double dt, double ekin, double virial) {
+    double const pv = R->baro_P * volume(R->h);
+    R->p_eps += (2. * R->alpha * ekin + 3. * virial - 3. * pv) * dt;
+}
+
+__device__ int monomial_index(int iv, int ivp) {
+    constexpr int VA[6] = {0, 1, 2, 1, 0, 0}, VB[6] = {0, 1, 2, 2, 2, 1};
+    // exponents (x, y, z) of the monomials in the order the force kernel accumulates them
+    constexpr int EX[15][3] = {{4, 0, 0}, {0, 4, 0}, {0, 0, 4}, {3, 1, 0}, {3, 0, 1},
+                               {1, 3, 0}, {0, 3, 1}, {1, 0, 3}, {0, 1, 3}, {2, 2, 0},
+                               {2, 0, 2}, {0, 2, 2}, {2, 1, 1}, {1, 2, 1}, {1, 1, 2}};
+    int e[3] = {0, 0, 0};
+    e[VA[iv]]++;
+    e[VB[iv]]++;
+    e[VA[ivp]]++;
+    e[VB[ivp]]++;
+    for (int m = 0; m < 15; ++m)
+        if (EX[m][0] == e[0] && EX[m][1] == e[1] && EX[m][2] == e[2])
+            return m;
+    return 0;
+}
+
+} // namespace
+
+// Opening scalar work of integrate() (md_driver.cpp:567-581): barostat and particle NHC
+// half steps, U2p, and the coefficients of the opening kick and of the drift, with the
+// NPT box update of U1 (md_driver.cpp:488-498).
+__global__ void k_pre(AtomsView A) {
+    Replica *R = A.rep + blockIdx.x;
+    __shared__ double s_S, s_ekin;
+    int const ens = R->ensemble;
+    double const dt = R->dt;
+    if (threadIdx.x == 0) {
+        double ekin = R->obs.ekin_tot;
+        double S = 1.;
+        if (ens == MDELAST_NVT || ens == MDELAST_NPT) {
+            S = nhc_thermo(R, R->th, 0.5 * dt, ekin);
+        }
+        s_S = S;
+        s_ekin = ekin;
+    } else if (threadIdx.x == 32 && ens == MDELAST_NPT) {
+        nhc_baro(R, R->bth, 0.5 * dt);
+    }
+    __syncthreads();
+    if (threadIdx.x != 0)
+        return;
+    double const ekin = s_ekin;
+    R->obs.ekin_tot = ekin;
+    double e = 1., c = 1.;
+    if (ens == MDELAST_NPT) {
+        U2p(R, 0.5 * dt, ekin, R->obs.virial);
+        double const x = R->alpha * (0.5 * dt) * R->p_eps / R->baro_w;
+        expx_operator(x, e, c);
+    }
+    R->s_kick = R->vscale * s_S;
+    R->vscale = 1.;
+    R->e_kick = e;
+    R->cdt_kick = c * (0.5 * dt);
+    // U1 (md_driver.cpp:464-470, 488-498)
+    double cf = 1.;
+    if (ens == MDELAST_NPT) {
+        double const x = dt * R->p_eps / R->baro_w;
+        R->eps += x;
+        double ee;
+        expx_operator(x, ee, cf);
+    }
+    R->cfdt = cf * dt;
+    for (int a = 0; a < 3; ++a)
+        R->h_pos[a] = R->h[a];
+    if (ens == MDELAST_NPT) {
+        double const expe = exp(R->eps);
+        double const vol_old = volume(R->h);
+        for (int a = 0; a < 3; ++a)
+            R->h[a] = R->h0[a] * expe;
+        if (fabs(volume(R->h) / vol_old - 1.) > 0.05)
+            atomicOr(&R->obs.status, MDELAST_FATAL_VOLUME);
+    }
+}
+
+// Closing scalar work: reduce the block sums of the density and force passes, finish
+// calculate_forces (md_driver.cpp:410-429), the tail of U2 (set_kinetic_energies,
+// calculate_configurational_temperature), U2p and the NHC half steps (md_driver.cpp:
+// 583-595), and calculate_thermodynamics (md_driver.cpp:648-730). POST_INIT does the
+// part of the constructor after calculate_forces (md_driver.cpp:114-118).
+__global__ void k_post(AtomsView A, int mode, int obs) {
+    Replica *R = A.rep + blockIdx.x;
+    __shared__ double sf[F_NSUM], sd[D_NSUM];
+    __shared__ double s_part[4][F_NSUM + D_NSUM];
+    __shared__ double s_S, s_ekin, s_virial;
+    int const t = threadIdx.x;
+    // Block sums of the two passes: 4 groups of 64 threads, thread (g, q) adds slot q over
+    // blocks g, g+4, ... with four independent accumulators; the group totals are then
+    // added in a fixed order, so the result does not depend on timing.
+    {
+        int const g = t >> 6, q = t & 63;
+        int const nslot = F_NSUM + D_NSUM;
+        if (q < nslot) {
+            bool const fpass = q < F_NSUM;
+            int const ns = fpass ? F_NSUM : D_NSUM;
+            int const col = fpass ? q : q - F_NSUM;
+            double const *P = fpass ? A.pf : A.pd;
+            long const b0 = fpass ? R->fblk_begin : R->dblk_begin;
+            int const nb = fpass ? R->fblk_n : R->dblk_n;
+            double a0 = 0., a1 = 0., a2 = 0., a3 = 0.;
+            int b = g;
+            for (; b + 12 < nb; b += 16) {
+                a0 += P[(b0 + b) * ns + col];
+                a1 += P[(b0 + b + 4) * ns + col];
+                a2 += P[(b0 + b + 8) * ns + col];
+                a3 += P[(b0 + b + 12) * ns + col];
+            }
+            for (; b < nb; b += 4)
+                a0 += P[(b0 + b) * ns + col];
+            s_part[g][q] = (a0 + a1) + (a2 + a3);
+        }
+        __syncthreads();
+        if (t < nslot) {
+            double const v = (s_part[0][t] + s_part[1][t]) + (s_part[2][t] + s_part[3][t]);
+            if (t < F_NSUM)
+                sf[t] = v;
+            else
+                sd[t - F_NSUM] = v;
+        }
+    }
+    __syncthreads();
+    int const ens = R->ensemble;
+    double const dt = R->dt;
+    mdelast_observables &o = R->obs;
+    if (t == 0) {
+        double const virial = sf[F_VIRIAL] / -3.;
+        s_virial = virial;
+        o.virial = virial;
+        double const vir_trace = -(sf[F_SIGMA] + sf[F_SIGMA + 1] + sf[F_SIGMA + 2]);
+        if (fabs(virial / (vir_trace / 3.) - 1.) > 1e-7)
+            atomicOr(&o.status, MDELAST_WARN_VIRIAL);
+        if (obs) {
+            double const lap = sf[F_LAP] + sd[D_LAP];
+            o.total_laplacian = lap;
+            int q = 0;
+            for (int a = 0; a < 6; ++a)
+                for (int b = 0; b < 6; ++b) {
+                    if (b < a) {
+                        o.born_elasticity_tensor[6 * a + b] = 0.;
+                        continue;
+                    }
+                    o.born_elasticity_tensor[6 * a + b] =
+                        sf[F_CB + monomial_index(a, b)] + sd[D_CB + q];
+                    ++q;
+                }
+        }
+        double ekin = sf[F_EKIN];
+        if (mode == POST_STEP) {
+            if (obs) {
+                double const f2 = sf[F_F2];
+                o.total_force2 = f2;
+                o.temperature_conf_inverse =
+                    (f2 != 0. && o.total_laplacian != 0.) ? kBoltz * o.total_laplacian / f2 : 0.;
+            }
+            if (ens == MDELAST_NPT)
+                U2p(R, 0.5 * dt, ekin, virial);
+        }
+        s_ekin = ekin;
+    }
+    __syncthreads();
+    if (mode == POST_STEP) {
+        if (t == 0) {
+            double ekin = s_ekin, S = 1.;
+            if (ens == MDELAST_NVT || ens == MDELAST_NPT) {
+                S = nhc_thermo(R, R->th, 0.5 * dt, ekin);
+            }
+            s_S = S;
+            s_ekin = ekin;
+        } else if (t == 32 && ens == MDELAST_NPT) {
+            nhc_baro(R, R->bth, 0.5 * dt);
+        }
+    } else if (t == 0) {
+        s_S = 1.;
+    }
+    __syncthreads();
+    if (t != 0)
+        return;
+    // calculate_thermodynamics (md_driver.cpp:648-730)
+    double const S = s_S, ekin = s_ekin, virial = s_virial;
+    int const N = R->n_atoms;
+    R->vscale = S;
+    o.ekin_tot = ekin;
+    o.ekin_atom = ekin / N;
+    double mom2 = 0.;
+    for (int a = 0; a < 3; ++a) {
+        o.momentum_tot[a] = S * sf[F_MV + a];
+        mom2 += o.momentum_tot[a] * o.momentum_tot[a];
+    }
+    if (mom2 / (2. * R->mass0 * ekin) > 1e-14)
+        atomicOr(&o.status, MDELAST_FATAL_MOMENTUM);
+    o.epot_atom = sf[F_EPOT] / N;
+    o.epot_eam_atom = sd[D_FSUM] / N;
+    o.etot_atom = o.ekin_atom + o.epot_atom;
+    double const old = o.etot_cons;
+    double etot = o.etot_atom * N;
+    if (ens == MDELAST_NVT || ens == MDELAST_NPT)
+        etot += chain_etot(R->th);
+    double const V = volume(R->h);
+    if (ens == MDELAST_NPT)
+        etot += V * R->baro_P + (0.5 * (R->p_eps * R->p_eps) / R->baro_w + chain_etot(R->bth));
+    o.etot_cons = etot;
+    double const e0 = mode == POST_INIT ? 0. : R->etot_cons_initial;
+    o.etot_cons_err = fabs(etot / e0 - 1.);
+    double const err_current = fabs(etot / old - 1.);
+    o.temperature_kin = 2. * ekin / (kBoltz * R->Nf);
+    if (obs) {
+        double const f2 = sf[F_F2];
+        o.total_force2 = f2;
+        o.temperature_conf_inverse =
+            (f2 != 0. && o.total_laplacian != 0.) ? kBoltz * o.total_laplacian / f2 : 0.;
+    }
+    o.pressure = (ekin * 2. / 3. + virial) / V;
+    double const S2 = S * S;
+    for (int k = 0; k < 6; ++k) {
+        o.stress_tensor[k] = (-sf[F_SIGMA + k] + S2 * sf[F_MVV + k]) / V;
+        o.born_stress_tensor[k] = sf[F_SIGMA + k] / V;
+    }
+    if (obs)
+        for (int k = 0; k < 36; ++k)
+            o.born_elasticity_tensor[k] /= V;
+    double const p_trace = o.stress_tensor[0] + o.stress_tensor[1] + o.stress_tensor[2];
+    if (fabs(o.pressure / (p_trace / 3.) - 1.) > 1e-5)
+        atomicOr(&o.status, MDELAST_FATAL_PRESSURE);
+    if ((o.etot_cons_err > R->fatal_conservation || err_current > R->fatal_conservation) &&
+        R->cycle > 0.)
+        atomicOr(&o.status, MDELAST_FATAL_CONSERVATION);
+    if (mode == POST_STEP) {
+        R->time += dt;
+        R->cycle += 1.;
+    } else {
+        R->etot_cons_initial = etot;
+        o.etot_cons_initial = etot;
+    }
+    o.etot_cons_initial = R->etot_cons_initial;
+    o.time = R->time;
+    o.cycle = R->cycle;
+    for (int a = 0; a < 3; ++a) {
+        for (int b = 0; b < 3; ++b)
+            o.box[3 * a + b] = a == b ? R->h[a] : 0.;
+    }
+    o.baro_epsilon = R->eps;
+    o.baro_p_epsilon = R->p_eps;
+    o.sample_observables = obs;
+}
+
+} // namespace mdelast
