@@ -189,6 +189,21 @@ void mdelast_driver_destroy(mdelast_driver *d);
 int mdelast_driver_integrate(mdelast_driver *d, int32_t n_steps);
 /* MDDriver::calculate_neighbors() (md_driver.cpp:279-298) */
 int mdelast_driver_calculate_neighbors(mdelast_driver *d);
+/* n_steps of the run loop of molecular_dynamics.py:1240-1254 without its Python: before the
+ * step that starts at cycle c the list is rebuilt when rebuild_every > 0 and
+ * c % rebuild_every == 0 (drivers with neighbors=1), and the step samples the Born tensor
+ * and Laplacian when sample_every > 0 and (c + 1) % sample_every == 0. The rebuilds run on
+ * the device inside the step graph with the current capacities (an overflow is reported
+ * like a FATAL). If device_ms is not NULL the call waits for the steps and stores their
+ * duration measured with CUDA events on the driver's stream. */
+int mdelast_driver_run(mdelast_driver *d, int32_t n_steps, int32_t rebuild_every,
+                       int32_t sample_every, float *device_ms);
+/* Diagnostics: run n_steps sampled steps with a CUDA event between consecutive kernels
+ * and store the mean device time per launch, in ms, of each kernel of the step:
+ * [0] opening scalar work, [1] kick + drift, [2] density pass, [3] force pass + kick,
+ * [4] closing scalar work, [5] neighbour-list build. */
+#define MDELAST_N_KERNEL_TIMES 6
+int mdelast_driver_kernel_times(mdelast_driver *d, int32_t n_steps, double *ms_out);
 /* the sample_observables flag (md_driver.hpp:163-167) */
 int mdelast_driver_set_sample_observables(mdelast_driver *d, int32_t flag);
 int mdelast_driver_get_sample_observables(const mdelast_driver *d, int32_t *flag);

@@ -4,41 +4,10 @@
 // The full neighbour list makes the pair passes gather-only: no atomics, deterministic
 // results, and forces that are antisymmetric pair by pair to the last bit.
 #include "kernels.cuh"
+#include "pair_common.cuh"
 
 namespace mdelast {
 
-namespace {
-
-__device__ __forceinline__ void status_or(Replica *rep, unsigned bits) {
-    atomicOr(&rep->obs.status, bits);
-}
-
-// Block-wide sum of NS per-thread values into out[0..NS) (thread 0 writes), warp shuffles
-// then shared memory; deterministic for a fixed block size.
-template <int NS>
-__device__ __forceinline__ void block_sum_store(double (&v)[NS], double *out) {
-    __shared__ double sm[kBlock / 32][NS];
-    int const lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int k = 0; k < NS; ++k) {
-        double x = v[k];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1)
-            x += __shfl_down_sync(0xffffffffu, x, o);
-        if (lane == 0)
-            sm[warp][k] = x;
-    }
-    __syncthreads();
-    for (int k = threadIdx.x; k < NS; k += blockDim.x) {
-        double s = 0.;
-#pragma unroll
-        for (int w = 0; w < kBlock / 32; ++w)
-            s += sm[w][k];
-        out[k] = s;
-    }
-}
-
-} // namespace
 
 // ------------------------------------------------------------------------------------
 // neighbour list (md_driver.cpp:279-298): every pair with the reference's min-image
@@ -199,25 +168,6 @@ __global__ void k_nbr_build(AtomsView A) {
 // so those per-atom Born and Laplacian terms (md_driver.cpp:410-419) are formed here and
 // g, h are never stored.
 
-// TPA lanes (a power of two dividing 32) share one atom: lane `sub` takes the atom's list
-// entries sub, sub + TPA, ... and the per-atom sums are combined across the lanes with
-// shuffles. TPA > 1 gives a small cell enough threads to cover the GPU; a large batch of
-// replicas runs with TPA = 1. Every lane reaches the shuffles (padding lanes add zeros).
-template <int TPA> __device__ __forceinline__ double group_sum(double x) {
-#pragma unroll
-    for (int o = TPA / 2; o > 0; o >>= 1)
-        x += __shfl_xor_sync(0xffffffffu, x, o);
-    return x;
-}
-
-__device__ __forceinline__ int list_slot(int kk, int nu, int maxn) {
-    return kk < nu ? kk : maxn - 1 - (kk - nu);
-}
-
-// Work split: the blocks of a pass are dealt out to the replicas (A.dblk_rep / fblk_rep);
-// block lb of a replica with nb blocks takes atom groups lb, lb + nb, ... of kBlock/TPA
-// atoms, so a block's partial sums belong to one replica and the block-wide reduction at
-// the end is paid once for several groups.
 template <bool OBS, int TPA>
 __global__ void __launch_bounds__(kBlock) k_density(AtomsView A, TablesView T) {
     int const r = A.dblk_rep[blockIdx.x];
@@ -242,9 +192,12 @@ __global__ void __launch_bounds__(kBlock) k_density(AtomsView A, TablesView T) {
         int const ti = static_cast<int>(ci.w);
         int const nu = A.n_up[i], ntot = nu + A.n_dn[i];
         int const *row = A.nbr + static_cast<size_t>(i) * A.maxn;
+        // the next partner's index and record are loaded one iteration ahead
+        double4 cn = A.crd[sub < ntot ? row[list_slot(sub, nu, A.maxn)] : i];
         for (int kk = sub; kk < ntot; kk += TPA) {
-            int const j = row[list_slot(kk, nu, A.maxn)];
-            double4 const cj = A.crd[j];
+            double4 const cj = cn;
+            if (kk + TPA < ntot)
+                cn = A.crd[row[list_slot(kk + TPA, nu, A.maxn)]];
             double px, py, pz;
             double const r2 = min_image_r2(ci, cj, hx, hy, hz, px, py, pz);
             if (r2 > T.r_cut_sq)
@@ -350,10 +303,19 @@ __global__ void __launch_bounds__(kBlock) k_force(AtomsView A, TablesView T) {
         int const nu = A.n_up[i], ntot = nu + A.n_dn[i];
         int const *row = A.nbr + static_cast<size_t>(i) * A.maxn;
         bool warn_rmin = false;
+        // the next partner's index, record and F' are loaded one iteration ahead
+        int jn = sub < ntot ? row[list_slot(sub, nu, A.maxn)] : i;
+        double4 cn = A.crd[jn];
+        double2 fn = A.dF2[jn];
         for (int kk = sub; kk < ntot; kk += TPA) {
             bool const upper = kk < nu;
-            int const j = row[list_slot(kk, nu, A.maxn)];
-            double4 const cj = A.crd[j];
+            double4 const cj = cn;
+            double2 const dFj2 = fn;
+            if (kk + TPA < ntot) {
+                jn = row[list_slot(kk + TPA, nu, A.maxn)];
+                cn = A.crd[jn];
+                fn = A.dF2[jn];
+            }
             double px, py, pz;
             double const r2 = min_image_r2(ci, cj, hx, hy, hz, px, py, pz);
             if (r2 > T.r_cut_sq)
@@ -401,7 +363,6 @@ __global__ void __launch_bounds__(kBlock) k_force(AtomsView A, TablesView T) {
                     if (OBS)
                         d2rho_j = tab_d2(c, t, T.inv_hr2);
                 }
-                double2 const dFj2 = A.dF2[j];
                 double const dFj = dFj2.x;
                 // the two cross terms are rounded separately and added (commutative), so
                 // the i- and j-side evaluations of dE/dr are bitwise equal
@@ -527,6 +488,11 @@ __global__ void __launch_bounds__(kBlock) k_kick_drift(AtomsView A, TablesView T
     c.y = __dadd_rn(c.y, __ddiv_rn(__dmul_rn(a, v[1]), R->h_pos[1]));
     c.z = __dadd_rn(c.z, __ddiv_rn(__dmul_rn(a, v[2]), R->h_pos[2]));
     A.crd[i] = c;
+    if (A.posf) // mixed precision: wrapped FP32 positions in the box after this drift
+        A.posf[i] = make_float4(static_cast<float>((c.x - nint_ref(c.x)) * R->h[0] / kAng),
+                                static_cast<float>((c.y - nint_ref(c.y)) * R->h[1] / kAng),
+                                static_cast<float>((c.z - nint_ref(c.z)) * R->h[2] / kAng),
+                                static_cast<float>(c.w));
 }
 
 // ------------------------------------------------------------------------------------

@@ -89,7 +89,18 @@ struct TablesView {
     double eam_rcut[kMaxTypes];
     double rhomax[kMaxTypes];
     double mass[kMaxTypes];
+    // mixed precision: the r bundles in FP32 with lengths in angstrom and values in eV
+    // (phi) or angstrom^-3 (rho); cutoffs in angstrom
+    const float *rbf;
+    float finv_hr, finv_hr2, fr_cut_sq, fpad;
+    float fpot_rcut[kMaxTypes * (kMaxTypes + 1) / 2];
+    float fpot_rmin[kMaxTypes * (kMaxTypes + 1) / 2];
+    float feam_rcut[kMaxTypes];
 };
+
+// cgs <-> the angstrom / eV units of the mixed-precision kernels (units.hpp:6-24)
+constexpr double kEv = 1.6021773e-12;
+constexpr double kAng = 1e-8;
 
 struct AtomsView {
     int n_pad, n_rep;
@@ -99,6 +110,8 @@ struct AtomsView {
     double *vel, *frc; // [3][n_pad]
     double *rho, *Fe, *epot;
     double2 *dF2;
+    float4 *posf; // mixed precision: wrapped positions [angstrom], type in .w (or null)
+    float2 *dF2f; // mixed precision: F' [eV A^3], F'' [eV A^6]
     int *nbr, *n_up, *n_dn;
     int maxn;
     double *pd, *pf; // per-block partial sums [n_blocks][D_NSUM], [n_blocks][F_NSUM]

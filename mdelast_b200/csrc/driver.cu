@@ -59,10 +59,11 @@ int default_tpa(int n_atoms) {
 }
 
 // Deal the blocks of a pair pass out to the replicas in proportion to their atom counts:
-// about kTargetBlocks in all (a few resident waves on 148 SMs), never fewer than one per
-// replica nor more than one per atom group of kBlock/tpa atoms. Fills each replica's block
-// range and the block -> replica map; returns the grid size.
-constexpr int kTargetBlocks = 148 * 4;
+// at most kTargetBlocks in all (many resident waves on 148 SMs: a block then loops over
+// several atom groups only for large batches), never fewer than one per replica nor more
+// than one per atom group of kBlock/tpa atoms. Fills each replica's block range and the
+// block -> replica map; returns the grid size.
+constexpr int kTargetBlocks = 148 * 32;
 
 int deal_blocks(std::vector<Replica *> const &reps, int tpa, bool density,
                 std::vector<int> &blk_rep) {
@@ -126,6 +127,22 @@ struct mdelast_driver_s {
     double *d_vel = nullptr, *d_frc = nullptr, *d_rho = nullptr, *d_Fe = nullptr,
            *d_epot = nullptr;
     double2 *d_dF2 = nullptr;
+    int precision = MDELAST_PRECISION_FP64;
+    float4 *d_posf = nullptr;
+    float2 *d_dF2f = nullptr;
+    float *d_rbf = nullptr;
+    void pass_density(bool obs, cudaStream_t s) {
+        if (precision == MDELAST_PRECISION_MIXED)
+            launch_density_mx(obs, tpa_d, grid_d, s, A, T);
+        else
+            launch_density(obs, tpa_d, grid_d, s, A, T);
+    }
+    void pass_force(bool obs, bool kick, cudaStream_t s) {
+        if (precision == MDELAST_PRECISION_MIXED)
+            launch_force_mx(obs, kick, tpa_f, grid_f, s, A, T);
+        else
+            launch_force(obs, kick, tpa_f, grid_f, s, A, T);
+    }
     int *d_nbr = nullptr, *d_nup = nullptr, *d_ndn = nullptr;
     double *d_pd = nullptr, *d_pf = nullptr;
     int *d_cell_count = nullptr, *d_cell_atoms = nullptr, *d_max_count = nullptr;
@@ -138,7 +155,8 @@ struct mdelast_driver_s {
     TablesView T{};
     mdelast_observables *h_obs = nullptr; // pinned, n_rep entries
     cudaEvent_t ev_step = nullptr;
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr}; // [2 * rebuild + obs]
+    unsigned long long host_cycle = 0; // steps launched (the reference's cycle counter)
     bool all_pairs = false; // every replica lists by all-pairs search
 
     ~mdelast_driver_s();
@@ -149,7 +167,9 @@ struct mdelast_driver_s {
     int configure_cells(double const h[3]);
     int enqueue_rebuild();
     int build_list_checked();
-    int enqueue_step(int obs);
+    int enqueue_step(int obs, int rebuild);
+    int step_graph(int obs, int rebuild, cudaGraphExec_t *out);
+    int launch_steps(int n_steps, int rebuild_every, int sample_every);
     int wait_step();
     int check_status();
 };
@@ -173,6 +193,9 @@ mdelast_driver_s::~mdelast_driver_s() {
     dfree(d_Fe);
     dfree(d_epot);
     dfree(d_dF2);
+    dfree(d_posf);
+    dfree(d_dF2f);
+    dfree(d_rbf);
     dfree(d_nbr);
     dfree(d_nup);
     dfree(d_ndn);
@@ -304,20 +327,66 @@ int mdelast_driver_s::build_list_checked() {
     return fail(MDELAST_ERR_CAPACITY, "neighbour list did not fit after repeated growth");
 }
 
-int mdelast_driver_s::enqueue_step(int obs) {
+int mdelast_driver_s::enqueue_step(int obs, int rebuild) {
     int const grid = n_pad / kBlock;
+    if (rebuild && neighbors) // calculate_neighbors() before integrate() (md.py:1245-1251)
+        if (int rc = enqueue_rebuild())
+            return rc;
     k_pre<<<n_rep, 64, 0, stream>>>(A);
     k_kick_drift<<<grid, kBlock, 0, stream>>>(A, T);
     if (!neighbors)
         if (int rc = enqueue_rebuild())
             return rc;
-    launch_density(obs != 0, tpa_d, grid_d, stream, A, T);
-    launch_force(obs != 0, true, tpa_f, grid_f, stream, A, T);
+    pass_density(obs != 0, stream);
+    pass_force(obs != 0, true, stream);
     k_post<<<n_rep, 256, 0, stream>>>(A, POST_STEP, obs);
     CK(cudaGetLastError());
     CK(cudaMemcpy2DAsync(h_obs, sizeof(mdelast_observables),
                          reinterpret_cast<char *>(d_rep) + offsetof(Replica, obs), sizeof(Replica),
                          sizeof(mdelast_observables), n_rep, cudaMemcpyDeviceToHost, stream));
+    return MDELAST_OK;
+}
+
+// The instantiated graph of one step, captured on first use.
+int mdelast_driver_s::step_graph(int obs, int rebuild, cudaGraphExec_t *out) {
+    cudaGraphExec_t &ge = graph[2 * (rebuild ? 1 : 0) + (obs ? 1 : 0)];
+    if (!ge) {
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        int rc = enqueue_step(obs, rebuild);
+        cudaError_t e = cudaStreamEndCapture(stream, &g);
+        if (rc)
+            return rc;
+        if (e != cudaSuccess)
+            return fail(MDELAST_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&ge, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess)
+            return fail(MDELAST_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    }
+    *out = ge;
+    return MDELAST_OK;
+}
+
+// Launch n steps; rebuild_every / sample_every < 0 mean "never" / "use the flag".
+int mdelast_driver_s::launch_steps(int n_steps, int rebuild_every, int sample_every) {
+    for (int s = 0; s < n_steps; ++s) {
+        unsigned long long const c = host_cycle;
+        int const rebuild = rebuild_every > 0 && c % static_cast<unsigned>(rebuild_every) == 0;
+        int const obs = sample_every < 0 ? sample
+                                         : (sample_every > 0 &&
+                                            (c + 1) % static_cast<unsigned>(sample_every) == 0);
+        cudaGraphExec_t g;
+        if (int rc = step_graph(obs, rebuild, &g))
+            return rc;
+        CK(cudaGraphLaunch(g, stream));
+        ++host_cycle;
+    }
+    if (n_steps > 0) {
+        CK(cudaEventRecord(ev_step, stream));
+        obs_valid = false;
+        stepped = true;
+    }
     return MDELAST_OK;
 }
 
@@ -384,8 +453,8 @@ int mdelast_driver_create(const mdelast_driver_config *cfg, mdelast_driver **out
         for (int b = 0; b < 3; ++b)
             if (a != b && c.box[3 * a + b] != 0.)
                 return fail(MDELAST_ERR_ARGUMENT, "the box must be diagonal");
-    if (c.precision != MDELAST_PRECISION_FP64)
-        return fail(MDELAST_ERR_UNSUPPORTED, "precision %d is not available", c.precision);
+    if (c.precision != MDELAST_PRECISION_FP64 && c.precision != MDELAST_PRECISION_MIXED)
+        return fail(MDELAST_ERR_ARGUMENT, "precision %d is not defined", c.precision);
     // tables: every pair slot and EAM function on one r grid
     mdelast_pair const *p0 = c.pair[0];
     for (int s = 0; s < npot; ++s) {
@@ -505,6 +574,27 @@ int mdelast_driver_create(const mdelast_driver_config *cfg, mdelast_driver **out
         T.rhomax[t] = c.n_eam ? c.eam[t]->rhomax_fatal : 0.;
         T.mass[t] = c.mass[t];
     }
+    d->precision = c.precision;
+    if (c.precision == MDELAST_PRECISION_MIXED) {
+        // the r bundles in FP32, angstrom / eV (phi) and angstrom^-3 (rho)
+        std::vector<float> rbf(rb.size());
+        double const a3 = kAng * kAng * kAng;
+        for (size_t q = 0; q < rb.size(); ++q)
+            rbf[q] = static_cast<float>(rb[q] * ((q % 18) < 6 ? 1. / kEv : a3));
+        TRY(dalloc(&d->d_rbf, rbf.size()));
+        if (cudaMemcpy(d->d_rbf, rbf.data(), sizeof(float) * rbf.size(), cudaMemcpyHostToDevice))
+            return bail(fail(MDELAST_ERR_CUDA, "table upload failed"));
+        T.rbf = d->d_rbf;
+        T.finv_hr = static_cast<float>(T.inv_hr * kAng);
+        T.finv_hr2 = static_cast<float>(T.inv_hr2 * kAng * kAng);
+        T.fr_cut_sq = static_cast<float>((rcut / kAng) * (rcut / kAng));
+        for (int s = 0; s < npot; ++s) {
+            T.fpot_rcut[s] = static_cast<float>(T.pot_rcut[s] / kAng);
+            T.fpot_rmin[s] = static_cast<float>(T.pot_rmin[s] / kAng);
+        }
+        for (int t = 0; t < nt; ++t)
+            T.feam_rcut[t] = static_cast<float>(T.eam_rcut[t] / kAng);
+    }
 
     // ---- replica state
     Replica R;
@@ -572,6 +662,10 @@ int mdelast_driver_create(const mdelast_driver_config *cfg, mdelast_driver **out
     TRY(dalloc(&d->d_Fe, np));
     TRY(dalloc(&d->d_epot, np));
     TRY(dalloc(&d->d_dF2, np));
+    if (c.precision == MDELAST_PRECISION_MIXED) {
+        TRY(dalloc(&d->d_posf, np));
+        TRY(dalloc(&d->d_dF2f, np));
+    }
     TRY(dalloc(&d->d_nup, np));
     TRY(dalloc(&d->d_ndn, np));
     TRY(dalloc(&d->d_pd, static_cast<size_t>(d->grid_d) * D_NSUM));
@@ -600,6 +694,8 @@ int mdelast_driver_create(const mdelast_driver_config *cfg, mdelast_driver **out
     A.Fe = d->d_Fe;
     A.epot = d->d_epot;
     A.dF2 = d->d_dF2;
+    A.posf = d->d_posf;
+    A.dF2f = d->d_dF2f;
     A.n_up = d->d_nup;
     A.n_dn = d->d_ndn;
     A.pd = d->d_pd;
@@ -623,8 +719,10 @@ int mdelast_driver_create(const mdelast_driver_config *cfg, mdelast_driver **out
 
     // ---- the constructor's force call and thermodynamics (md_driver.cpp:112-118)
     TRY(d->build_list_checked());
-    launch_density(true, d->tpa_d, d->grid_d, d->stream, d->A, d->T);
-    launch_force(true, false, d->tpa_f, d->grid_f, d->stream, d->A, d->T);
+    if (d->A.posf)
+        k_posf<<<np / kBlock, kBlock, 0, d->stream>>>(d->A);
+    d->pass_density(true, d->stream);
+    d->pass_force(true, false, d->stream);
     k_post<<<d->n_rep, 256, 0, d->stream>>>(d->A, POST_INIT, 1);
     if (cudaGetLastError() != cudaSuccess)
         return bail(fail(MDELAST_ERR_CUDA, "kernel launch failed"));
@@ -651,29 +749,98 @@ int mdelast_driver_integrate(mdelast_driver *d, int32_t n_steps) {
     if (d->dead)
         return d->check_status();
     CK(cudaSetDevice(d->device));
-    int const obs = d->sample ? 1 : 0;
-    if (!d->graph[obs]) {
-        cudaGraph_t g;
-        CK(cudaStreamBeginCapture(d->stream, cudaStreamCaptureModeThreadLocal));
-        int rc = d->enqueue_step(obs);
-        cudaError_t e = cudaStreamEndCapture(d->stream, &g);
-        if (rc)
+    return d->launch_steps(n_steps, -1, -1);
+}
+
+int mdelast_driver_run(mdelast_driver *d, int32_t n_steps, int32_t rebuild_every,
+                       int32_t sample_every, float *device_ms) {
+    clear_error();
+    if (!d || n_steps < 0)
+        return fail(MDELAST_ERR_ARGUMENT, "bad argument");
+    CK(cudaSetDevice(d->device));
+    if (int rc = d->wait_step())
+        return rc;
+    if (d->neighbors && rebuild_every > 0) { // cell geometry for the current box
+        double h[3] = {d->h_obs[0].box[0], d->h_obs[0].box[4], d->h_obs[0].box[8]};
+        if (int rc = d->configure_cells(h))
             return rc;
-        if (e != cudaSuccess)
-            return fail(MDELAST_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
-        e = cudaGraphInstantiate(&d->graph[obs], g, 0);
-        cudaGraphDestroy(g);
-        if (e != cudaSuccess)
-            return fail(MDELAST_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
     }
-    for (int s = 0; s < n_steps; ++s)
-        CK(cudaGraphLaunch(d->graph[obs], d->stream));
-    if (n_steps > 0) {
-        CK(cudaEventRecord(d->ev_step, d->stream));
-        d->obs_valid = false;
-        d->stepped = true;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (device_ms) {
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        CK(cudaEventRecord(e0, d->stream));
     }
-    return MDELAST_OK;
+    int rc = d->launch_steps(n_steps, d->neighbors ? rebuild_every : 0, sample_every);
+    if (device_ms && !rc) {
+        cudaEventRecord(e1, d->stream);
+        cudaError_t e = cudaEventSynchronize(e1);
+        if (e == cudaSuccess)
+            e = cudaEventElapsedTime(device_ms, e0, e1);
+        if (e != cudaSuccess)
+            rc = fail(MDELAST_ERR_CUDA, "step timing: %s", cudaGetErrorString(e));
+    }
+    if (e0)
+        cudaEventDestroy(e0);
+    if (e1)
+        cudaEventDestroy(e1);
+    return rc;
+}
+
+int mdelast_driver_kernel_times(mdelast_driver *d, int32_t n_steps, double *ms_out) {
+    clear_error();
+    if (!d || n_steps < 1 || !ms_out)
+        return fail(MDELAST_ERR_ARGUMENT, "bad argument");
+    CK(cudaSetDevice(d->device));
+    if (int rc = d->wait_step())
+        return rc;
+    std::vector<cudaEvent_t> ev(7);
+    for (auto &e : ev)
+        CK(cudaEventCreate(&e));
+    double acc[MDELAST_N_KERNEL_TIMES] = {0, 0, 0, 0, 0, 0};
+    int const grid = d->n_pad / kBlock;
+    cudaStream_t s = d->stream;
+    int rc = MDELAST_OK;
+    for (int step = 0; step < n_steps && !rc; ++step) {
+        cudaEventRecord(ev[0], s);
+        if (d->neighbors || step == 0)
+            rc = d->enqueue_rebuild();
+        cudaEventRecord(ev[1], s);
+        k_pre<<<d->n_rep, 64, 0, s>>>(d->A);
+        cudaEventRecord(ev[2], s);
+        k_kick_drift<<<grid, kBlock, 0, s>>>(d->A, d->T);
+        cudaEventRecord(ev[3], s);
+        d->pass_density(true, s);
+        cudaEventRecord(ev[4], s);
+        d->pass_force(true, true, s);
+        cudaEventRecord(ev[5], s);
+        k_post<<<d->n_rep, 256, 0, s>>>(d->A, POST_STEP, 1);
+        cudaEventRecord(ev[6], s);
+        cudaError_t e = cudaEventSynchronize(ev[6]);
+        if (e != cudaSuccess) {
+            rc = fail(MDELAST_ERR_CUDA, "kernel timing: %s", cudaGetErrorString(e));
+            break;
+        }
+        float t[6];
+        cudaEventElapsedTime(&t[5], ev[0], ev[1]);
+        for (int k = 0; k < 5; ++k)
+            cudaEventElapsedTime(&t[k], ev[k + 1], ev[k + 2]);
+        for (int k = 0; k < 6; ++k)
+            acc[k] += t[k];
+        ++d->host_cycle;
+    }
+    for (auto &e : ev)
+        cudaEventDestroy(e);
+    for (int k = 0; k < MDELAST_N_KERNEL_TIMES; ++k)
+        ms_out[k] = acc[k] / n_steps;
+    d->stepped = true;
+    CK(cudaMemcpy2D(d->h_obs, sizeof(mdelast_observables),
+                    reinterpret_cast<char *>(d->d_rep) + offsetof(Replica, obs), sizeof(Replica),
+                    sizeof(mdelast_observables), d->n_rep, cudaMemcpyDeviceToHost));
+    d->obs_valid = true;
+    if (rc)
+        return rc;
+    return d->check_status();
 }
 
 int mdelast_driver_calculate_neighbors(mdelast_driver *d) {

@@ -18,6 +18,12 @@ void launch_density(bool obs, int tpa, int grid, cudaStream_t s, AtomsView const
                     TablesView const &T);
 void launch_force(bool obs, bool kick, int tpa, int grid, cudaStream_t s, AtomsView const &A,
                   TablesView const &T);
+// the same passes with FP32 pair math (mixed precision)
+void launch_density_mx(bool obs, int tpa, int grid, cudaStream_t s, AtomsView const &A,
+                       TablesView const &T);
+void launch_force_mx(bool obs, bool kick, int tpa, int grid, cudaStream_t s, AtomsView const &A,
+                     TablesView const &T);
+__global__ void k_posf(AtomsView A);
 __global__ void k_kick_drift(AtomsView A, TablesView T);
 __global__ void k_pre(AtomsView A);
 __global__ void k_post(AtomsView A, int mode, int obs);

@@ -433,6 +433,16 @@ class MDDriver {
         }
     }
     void synchronize() { check(mdelast_driver_synchronize(d_)); }
+    double run(int n, int rebuild_every, int sample_every, bool timed) {
+        float ms = 0.f;
+        check(mdelast_driver_run(d_, n, rebuild_every, sample_every, timed ? &ms : nullptr));
+        return ms;
+    }
+    std::vector<double> kernel_times(int n) {
+        std::vector<double> t(MDELAST_N_KERNEL_TIMES);
+        check(mdelast_driver_kernel_times(d_, n, t.data()));
+        return t;
+    }
 
     Ensamble ensamble;
     ThermostatCoupling thermostat_coupling;
@@ -595,6 +605,14 @@ PYBIND11_MODULE(md_driver_module, m) {
         .def("atoms_array", &MDDriver::atoms_array, py::arg("field"))
         .def("neighbor_list", &MDDriver::neighbor_list)
         .def("synchronize", &MDDriver::synchronize)
+        .def("run", &MDDriver::run, py::arg("n_steps"), py::arg("rebuild_every") = 20,
+             py::arg("sample_every") = 1, py::arg("timed") = false,
+             "n_steps of the molecular_dynamics.py run loop on the device (list rebuild every "
+             "rebuild_every steps, observables every sample_every steps); returns the device "
+             "time in ms when timed")
+        .def("kernel_times", &MDDriver::kernel_times, py::arg("n_steps") = 10,
+             "mean device ms per launch: opening scalar, kick+drift, density, force, closing "
+             "scalar, list build")
         .def_readonly("precision", &MDDriver::precision_)
         .def_property_readonly("status", [](MDDriver &d) { return d.obs().status; });
 

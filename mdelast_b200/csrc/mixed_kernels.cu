@@ -1,0 +1,434 @@
+// Mixed-precision pair passes: pair geometry and table evaluation in FP32, in angstrom and
+// eV, with every sum over pairs (per-atom forces and energies, the virial, Born stress,
+// Born tensor and Laplacian) accumulated in FP64 and converted to cgs at the end.
+//
+// Pair forces stay exactly antisymmetric: dp_ij = -dp_ji bit for bit (IEEE subtraction and
+// round-to-nearest-even are odd functions), every other pair quantity depends on r only,
+// and the two EAM cross terms of dE/dr are rounded separately and added commutatively.
+// With the per-atom sums in FP64 the total momentum is conserved as in the FP64 path.
+//
+// The neighbour list, the embedding function and the integrator are shared with the FP64
+// path (FP64, cgs): the list comes from the FP64 coordinates, and k_kick_drift refreshes
+// the FP32 positions posf after every drift.
+#include "kernels.cuh"
+#include "pair_common.cuh"
+
+namespace mdelast {
+
+namespace {
+
+__device__ __forceinline__ int tab_locate_f(float x, float inv_h, int n, float &t) {
+    float const u = __fmul_rn(x, inv_h);
+    int i = 0;
+    if (u >= static_cast<float>(n))
+        i = n - 1;
+    else if (u > 0.f)
+        i = static_cast<int>(u);
+    t = u - static_cast<float>(i);
+    return i;
+}
+
+__device__ __forceinline__ void ld6f(const float *p, float c[6]) {
+    const float2 *q = reinterpret_cast<const float2 *>(p);
+    float2 a = __ldg(q), b = __ldg(q + 1), d = __ldg(q + 2);
+    c[0] = a.x;
+    c[1] = a.y;
+    c[2] = b.x;
+    c[3] = b.y;
+    c[4] = d.x;
+    c[5] = d.y;
+}
+
+__device__ __forceinline__ float tabf_v(const float *c, float t) {
+    return c[0] + t * (c[1] + t * (c[2] + t * (c[3] + t * (c[4] + t * c[5]))));
+}
+__device__ __forceinline__ float tabf_d1(const float *c, float t, float inv_h) {
+    return (c[1] + t * (2.f * c[2] + t * (3.f * c[3] + t * (4.f * c[4] + t * 5.f * c[5])))) * inv_h;
+}
+__device__ __forceinline__ float tabf_d2(const float *c, float t, float inv_h2) {
+    return (2.f * c[2] + t * (6.f * c[3] + t * (12.f * c[4] + t * 20.f * c[5]))) * inv_h2;
+}
+
+// minimum image of pi - pj in a box of edges L (positions wrapped into [-L/2, L/2))
+__device__ __forceinline__ float min_image_f(float4 pi, float4 pj, float3 L, float3 iL,
+                                             float &dx, float &dy, float &dz) {
+    dx = pi.x - pj.x;
+    dy = pi.y - pj.y;
+    dz = pi.z - pj.z;
+    dx -= L.x * rintf(dx * iL.x);
+    dy -= L.y * rintf(dy * iL.y);
+    dz -= L.z * rintf(dz * iL.z);
+    return dx * dx + dy * dy + dz * dz;
+}
+
+__device__ __forceinline__ void box_f(Replica const *R, float3 &L, float3 &iL) {
+    L = make_float3(static_cast<float>(R->h[0] / kAng), static_cast<float>(R->h[1] / kAng),
+                    static_cast<float>(R->h[2] / kAng));
+    iL = make_float3(1.f / L.x, 1.f / L.y, 1.f / L.z);
+}
+
+} // namespace
+
+// FP32 wrapped positions of every atom from the FP64 coordinates and the current box.
+__global__ void k_posf(AtomsView A) {
+    int const i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n_pad)
+        return;
+    int const r = A.rep_of[i];
+    if (r < 0)
+        return;
+    Replica const *R = A.rep + r;
+    double4 const c = A.crd[i];
+    A.posf[i] = make_float4(static_cast<float>((c.x - nint_ref(c.x)) * R->h[0] / kAng),
+                            static_cast<float>((c.y - nint_ref(c.y)) * R->h[1] / kAng),
+                            static_cast<float>((c.z - nint_ref(c.z)) * R->h[2] / kAng),
+                            static_cast<float>(c.w));
+}
+
+// Density pass of md_driver.cpp:195-277 in mixed precision (see k_density for the roles).
+template <bool OBS, int TPA>
+__global__ void __launch_bounds__(kBlock) k_density_mx(AtomsView A, TablesView T) {
+    int const r = A.dblk_rep[blockIdx.x];
+    Replica const *R = A.rep + r;
+    int const lb = blockIdx.x - R->dblk_begin, nb = R->dblk_n;
+    int const apb = kBlock / TPA, sub = threadIdx.x % TPA;
+    int const n_slots = R->n_blocks * kBlock;
+    float3 L, iL;
+    box_f(R, L, iL);
+    double acc[D_NSUM];
+#pragma unroll
+    for (int k = 0; k < D_NSUM; ++k)
+        acc[k] = 0.;
+    for (int a0 = lb * apb; a0 < n_slots; a0 += nb * apb) {
+        int const a = a0 + static_cast<int>(threadIdx.x) / TPA;
+        int const i = R->atom_begin + a;
+        bool const valid = a < R->n_atoms && T.has_eam;
+        float rho = 0.f;
+        float g[6] = {0, 0, 0, 0, 0, 0}, hv[3] = {0, 0, 0};
+        int ti = 0;
+        if (valid) {
+            float4 const pi = A.posf[i];
+            ti = static_cast<int>(pi.w);
+            int const nu = A.n_up[i], ntot = nu + A.n_dn[i];
+            int const *row = A.nbr + static_cast<size_t>(i) * A.maxn;
+            float4 pn = A.posf[sub < ntot ? row[list_slot(sub, nu, A.maxn)] : i];
+            for (int kk = sub; kk < ntot; kk += TPA) {
+                float4 const pj = pn;
+                if (kk + TPA < ntot)
+                    pn = A.posf[row[list_slot(kk + TPA, nu, A.maxn)]];
+                float dx, dy, dz;
+                float const r2 = min_image_f(pi, pj, L, iL, dx, dy, dz);
+                if (r2 > T.fr_cut_sq)
+                    continue;
+                float const dr = sqrtf(r2);
+                int const tj = static_cast<int>(pj.w);
+                if (dr > T.feam_rcut[tj])
+                    continue;
+                float t;
+                int const k = tab_locate_f(dr, T.finv_hr, T.nri, t);
+                int const off = (tj == (ti < tj ? ti : tj)) ? 6 : 12;
+                float c[6];
+                ld6f(T.rbf + (static_cast<size_t>(pair_slot(ti, tj)) * T.nri + k) * 18 + off, c);
+                rho += tabf_v(c, t);
+                if (OBS) {
+                    float const ar = tabf_d1(c, t, T.finv_hr) / dr;
+                    float const ap[3] = {ar * dx, ar * dy, ar * dz};
+                    g[0] += ap[0] * dx;
+                    g[1] += ap[1] * dy;
+                    g[2] += ap[2] * dz;
+                    g[3] += ap[1] * dz;
+                    g[4] += ap[0] * dz;
+                    g[5] += ap[0] * dy;
+                    hv[0] += ap[0];
+                    hv[1] += ap[1];
+                    hv[2] += ap[2];
+                }
+            }
+        }
+        rho = group_sum<TPA>(rho);
+        if (OBS) {
+#pragma unroll
+            for (int u = 0; u < 6; ++u)
+                g[u] = group_sum<TPA>(g[u]);
+#pragma unroll
+            for (int u = 0; u < 3; ++u)
+                hv[u] = group_sum<TPA>(hv[u]);
+        }
+        if (valid && sub == 0) {
+            // the embedding function in FP64 and cgs (eam.hpp:48-70)
+            double const rc = static_cast<double>(rho) / (kAng * kAng * kAng);
+            if (rc > T.rhomax[ti])
+                status_or(A.rep + r, MDELAST_FATAL_RHO_MAX);
+            double t;
+            int const k = tab_locate(rc, T.inv_hf, T.nfi, t);
+            double c[6];
+            ld6(T.Ft + (static_cast<size_t>(ti) * T.nfi + k) * 6, c);
+            double const F = tab_v(c, t), dF = tab_d1(c, t, T.inv_hf);
+            double const d2F = OBS ? tab_d2(c, t, T.inv_hf2) : 0.;
+            A.rho[i] = rc;
+            A.Fe[i] = F;
+            // F' [erg cm^3] -> [eV A^3] and F'' [erg cm^6] -> [eV A^6]
+            double const a3 = kAng * kAng * kAng;
+            if (OBS) {
+                A.dF2[i] = make_double2(dF, d2F);
+                A.dF2f[i] = make_float2(static_cast<float>(dF / (a3 * kEv)),
+                                        static_cast<float>(d2F / (a3 * a3 * kEv)));
+            } else {
+                A.dF2[i].x = dF;
+                A.dF2f[i].x = static_cast<float>(dF / (a3 * kEv));
+            }
+            acc[D_FSUM] += F;
+            if (OBS) {
+                // g in cm^-3 and h in cm^-4, as the cgs F'' expects
+                double gc[6], hc[3];
+#pragma unroll
+                for (int u = 0; u < 6; ++u)
+                    gc[u] = static_cast<double>(g[u]) / a3;
+#pragma unroll
+                for (int u = 0; u < 3; ++u)
+                    hc[u] = static_cast<double>(hv[u]) / (a3 * kAng);
+                int q = D_CB;
+#pragma unroll
+                for (int u = 0; u < 6; ++u)
+#pragma unroll
+                    for (int v = u; v < 6; ++v)
+                        acc[q++] += d2F * gc[u] * gc[v];
+                acc[D_LAP] += d2F * (hc[0] * hc[0] + hc[1] * hc[1] + hc[2] * hc[2]);
+            }
+        }
+    }
+    block_sum_store<D_NSUM>(acc, A.pd + static_cast<size_t>(blockIdx.x) * D_NSUM);
+}
+
+// Force pass of md_driver.cpp:300-430 (with the closing kick) in mixed precision; see
+// k_force for the roles of the terms.
+template <bool OBS, bool KICK, int TPA>
+__global__ void __launch_bounds__(kBlock) k_force_mx(AtomsView A, TablesView T) {
+    int const r = A.fblk_rep[blockIdx.x];
+    Replica const *R = A.rep + r;
+    int const lb = blockIdx.x - R->fblk_begin, nb = R->fblk_n;
+    int const apb = kBlock / TPA, sub = threadIdx.x % TPA;
+    int const n_slots = R->n_blocks * kBlock;
+    float3 L, iL;
+    box_f(R, L, iL);
+    double acc[F_NSUM];
+#pragma unroll
+    for (int k = 0; k < F_NSUM; ++k)
+        acc[k] = 0.;
+    for (int a0 = lb * apb; a0 < n_slots; a0 += nb * apb) {
+        int const a = a0 + static_cast<int>(threadIdx.x) / TPA;
+        int const i = R->atom_begin + a;
+        bool const valid = a < R->n_atoms;
+        double fx = 0., fy = 0., fz = 0., epot = 0.;
+        int ti = 0;
+        if (valid) {
+            float4 const pi = A.posf[i];
+            ti = static_cast<int>(pi.w);
+            float2 const dFi2 = T.has_eam ? A.dF2f[i] : make_float2(0.f, 0.f);
+            float const dFi = dFi2.x, d2Fi = OBS ? dFi2.y : 0.f;
+            int const nu = A.n_up[i], ntot = nu + A.n_dn[i];
+            int const *row = A.nbr + static_cast<size_t>(i) * A.maxn;
+            bool warn_rmin = false;
+            int jn = sub < ntot ? row[list_slot(sub, nu, A.maxn)] : i;
+            float4 pn = A.posf[jn];
+            float2 fn = A.dF2f[jn];
+            for (int kk = sub; kk < ntot; kk += TPA) {
+                bool const upper = kk < nu;
+                float4 const pj = pn;
+                float2 const dFj2 = fn;
+                if (kk + TPA < ntot) {
+                    jn = row[list_slot(kk + TPA, nu, A.maxn)];
+                    pn = A.posf[jn];
+                    fn = A.dF2f[jn];
+                }
+                float dx, dy, dz;
+                float const r2 = min_image_f(pi, pj, L, iL, dx, dy, dz);
+                if (r2 > T.fr_cut_sq)
+                    continue;
+                float const dr = sqrtf(r2);
+                float const idr = 1.f / dr;
+                int const tj = static_cast<int>(pj.w);
+                int const s = pair_slot(ti, tj);
+                float t;
+                int const k = tab_locate_f(dr, T.finv_hr, T.nri, t);
+                const float *bundle = T.rbf + (static_cast<size_t>(s) * T.nri + k) * 18;
+                float V = 0.f, dV = 0.f, d2V = 0.f;
+                if (dr < T.fpot_rmin[s])
+                    warn_rmin = true;
+                if (!(dr > T.fpot_rcut[s])) {
+                    float c[6];
+                    ld6f(bundle, c);
+                    V = tabf_v(c, t);
+                    dV = tabf_d1(c, t, T.finv_hr);
+                    if (OBS)
+                        d2V = tabf_d2(c, t, T.finv_hr2);
+                }
+                float dedr = dV, X = 0.f, lap = 0.f;
+                if (OBS) {
+                    X = d2V - dV * idr;
+                    lap = 2.f * (d2V + 2.f * dV * idr);
+                }
+                if (T.has_eam) {
+                    int const oi = (ti <= tj) ? 6 : 12, oj = (ti < tj) ? 12 : 6;
+                    float drho_i = 0.f, drho_j = 0.f, d2rho_i = 0.f, d2rho_j = 0.f;
+                    if (!(dr > T.feam_rcut[ti])) {
+                        float c[6];
+                        ld6f(bundle + oi, c);
+                        drho_i = tabf_d1(c, t, T.finv_hr);
+                        if (OBS)
+                            d2rho_i = tabf_d2(c, t, T.finv_hr2);
+                    }
+                    if (!(dr > T.feam_rcut[tj])) {
+                        float c[6];
+                        ld6f(bundle + oj, c);
+                        drho_j = tabf_d1(c, t, T.finv_hr);
+                        if (OBS)
+                            d2rho_j = tabf_d2(c, t, T.finv_hr2);
+                    }
+                    float const dFj = dFj2.x;
+                    dedr = __fadd_rn(dedr, __fadd_rn(__fmul_rn(dFi, drho_j), __fmul_rn(dFj, drho_i)));
+                    if (OBS) {
+                        float const d2Fj = dFj2.y;
+                        lap += 2.f * (dFj * (d2rho_i + 2.f * drho_i * idr) +
+                                      dFi * (d2rho_j + 2.f * drho_j * idr));
+                        lap += d2Fi * (drho_j * drho_j) + d2Fj * (drho_i * drho_i);
+                        X += dFi * (d2rho_j - drho_j * idr) + dFj * (d2rho_i - drho_i * idr);
+                    }
+                }
+                float const sc = __fmul_rn(-dedr, idr);
+                fx += static_cast<double>(__fmul_rn(sc, dx));
+                fy += static_cast<double>(__fmul_rn(sc, dy));
+                fz += static_cast<double>(__fmul_rn(sc, dz));
+                epot += static_cast<double>(0.5f * V);
+                if (upper) {
+                    acc[F_VIRIAL] += static_cast<double>(dr * dedr);
+                    float const xx = dx * dx, yy = dy * dy, zz = dz * dz;
+                    float const yz = dy * dz, xz = dx * dz, xy = dx * dy;
+                    float const w = dedr * idr;
+                    acc[F_SIGMA + 0] += static_cast<double>(w * xx);
+                    acc[F_SIGMA + 1] += static_cast<double>(w * yy);
+                    acc[F_SIGMA + 2] += static_cast<double>(w * zz);
+                    acc[F_SIGMA + 3] += static_cast<double>(w * yz);
+                    acc[F_SIGMA + 4] += static_cast<double>(w * xz);
+                    acc[F_SIGMA + 5] += static_cast<double>(w * xy);
+                    if (OBS) {
+                        X *= idr * idr;
+                        float const Xxx = X * xx, Xyy = X * yy, Xzz = X * zz;
+                        acc[F_CB + 0] += static_cast<double>(Xxx * xx);
+                        acc[F_CB + 1] += static_cast<double>(Xyy * yy);
+                        acc[F_CB + 2] += static_cast<double>(Xzz * zz);
+                        acc[F_CB + 3] += static_cast<double>(Xxx * xy);
+                        acc[F_CB + 4] += static_cast<double>(Xxx * xz);
+                        acc[F_CB + 5] += static_cast<double>(Xyy * xy);
+                        acc[F_CB + 6] += static_cast<double>(Xyy * yz);
+                        acc[F_CB + 7] += static_cast<double>(Xzz * xz);
+                        acc[F_CB + 8] += static_cast<double>(Xzz * yz);
+                        acc[F_CB + 9] += static_cast<double>(Xxx * yy);
+                        acc[F_CB + 10] += static_cast<double>(Xxx * zz);
+                        acc[F_CB + 11] += static_cast<double>(Xyy * zz);
+                        acc[F_CB + 12] += static_cast<double>(Xxx * yz);
+                        acc[F_CB + 13] += static_cast<double>(Xyy * xz);
+                        acc[F_CB + 14] += static_cast<double>(Xzz * xy);
+                        acc[F_LAP] += static_cast<double>(lap);
+                    }
+                }
+            }
+            if (warn_rmin)
+                status_or(A.rep + r, MDELAST_WARN_RMIN);
+        }
+        fx = group_sum<TPA>(fx);
+        fy = group_sum<TPA>(fy);
+        fz = group_sum<TPA>(fz);
+        epot = group_sum<TPA>(epot);
+        if (valid && sub == 0) {
+            double const kf = kEv / kAng; // eV/A -> dyn
+            fx *= kf;
+            fy *= kf;
+            fz *= kf;
+            epot *= kEv;
+            if (T.has_eam)
+                epot += A.Fe[i];
+            size_t const np = A.n_pad;
+            A.frc[i] = fx;
+            A.frc[np + i] = fy;
+            A.frc[np + i + np] = fz;
+            A.epot[i] = epot;
+            double const m = T.mass[ti];
+            double vx = A.vel[i], vy = A.vel[np + i], vz = A.vel[2 * np + i];
+            if (KICK) {
+                double const e = R->e_kick, cdt = R->cdt_kick;
+                vx = vx * e + cdt * fx / m;
+                vy = vy * e + cdt * fy / m;
+                vz = vz * e + cdt * fz / m;
+                A.vel[i] = vx;
+                A.vel[np + i] = vy;
+                A.vel[2 * np + i] = vz;
+            }
+            acc[F_F2] += fx * fx + fy * fy + fz * fz;
+            acc[F_EKIN] += 0.5 * m * (vx * vx + vy * vy + vz * vz);
+            acc[F_MVV + 0] += m * vx * vx;
+            acc[F_MVV + 1] += m * vy * vy;
+            acc[F_MVV + 2] += m * vz * vz;
+            acc[F_MVV + 3] += m * vy * vz;
+            acc[F_MVV + 4] += m * vx * vz;
+            acc[F_MVV + 5] += m * vx * vy;
+            acc[F_MV + 0] += vx * m;
+            acc[F_MV + 1] += vy * m;
+            acc[F_MV + 2] += vz * m;
+            acc[F_EPOT] += epot;
+        }
+    }
+    // pair sums from eV (and eV/A^2 for the Laplacian) to cgs
+    acc[F_VIRIAL] *= kEv;
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+        acc[F_SIGMA + k] *= kEv;
+#pragma unroll
+    for (int k = 0; k < 15; ++k)
+        acc[F_CB + k] *= kEv;
+    acc[F_LAP] *= kEv / (kAng * kAng);
+    block_sum_store<F_NSUM>(acc, A.pf + static_cast<size_t>(blockIdx.x) * F_NSUM);
+}
+
+namespace {
+template <bool OBS>
+void density_mx_tpa(int tpa, int grid, cudaStream_t s, AtomsView const &A, TablesView const &T) {
+    switch (tpa) {
+    case 1: k_density_mx<OBS, 1><<<grid, kBlock, 0, s>>>(A, T); break;
+    case 4: k_density_mx<OBS, 4><<<grid, kBlock, 0, s>>>(A, T); break;
+    case 8: k_density_mx<OBS, 8><<<grid, kBlock, 0, s>>>(A, T); break;
+    default: k_density_mx<OBS, 16><<<grid, kBlock, 0, s>>>(A, T); break;
+    }
+}
+template <bool OBS, bool KICK>
+void force_mx_tpa(int tpa, int grid, cudaStream_t s, AtomsView const &A, TablesView const &T) {
+    switch (tpa) {
+    case 1: k_force_mx<OBS, KICK, 1><<<grid, kBlock, 0, s>>>(A, T); break;
+    case 4: k_force_mx<OBS, KICK, 4><<<grid, kBlock, 0, s>>>(A, T); break;
+    case 8: k_force_mx<OBS, KICK, 8><<<grid, kBlock, 0, s>>>(A, T); break;
+    default: k_force_mx<OBS, KICK, 16><<<grid, kBlock, 0, s>>>(A, T); break;
+    }
+}
+} // namespace
+
+void launch_density_mx(bool obs, int tpa, int grid, cudaStream_t s, AtomsView const &A,
+                       TablesView const &T) {
+    if (obs)
+        density_mx_tpa<true>(tpa, grid, s, A, T);
+    else
+        density_mx_tpa<false>(tpa, grid, s, A, T);
+}
+
+void launch_force_mx(bool obs, bool kick, int tpa, int grid, cudaStream_t s, AtomsView const &A,
+                     TablesView const &T) {
+    if (obs && kick)
+        force_mx_tpa<true, true>(tpa, grid, s, A, T);
+    else if (obs)
+        force_mx_tpa<true, false>(tpa, grid, s, A, T);
+    else if (kick)
+        force_mx_tpa<false, true>(tpa, grid, s, A, T);
+    else
+        force_mx_tpa<false, false>(tpa, grid, s, A, T);
+}
+
+} // namespace mdelast

@@ -18,40 +18,47 @@ __constant__ double c_wsy7[7] = {
 
 constexpr double kBoltz = 1.38064852e-16; // units.hpp:7
 
-// exp(-x) and op(x) = (1 - exp(-x))/x of numerics.hpp:11-18. For |x| <= 1e-3, op is the
-// reference's own 5th-order Taylor polynomial. For |x| <= 1/16 both functions come from
-// their Taylor series, exp(-x) = sum (-x)^k/k! and op(x) = sum (-x)^k/(k+1)!, to degree 11
-// (the first omitted term is below 1e-23 relative), evaluated by Estrin's scheme: a
-// dependent chain of four FMAs instead of a library exp followed by a division, which
-// matters because the chain sweeps are sequential. For larger |x|, exp() and the
-// division as in the reference. Thermostat arguments are x = dt p_eta/Q ~ dt/tau, so the
-// series branch is the common one.
-__device__ __forceinline__ void expx_operator(double x, double &expx, double &op) {
-    double const ax = fabs(x);
-    if (ax <= 0.0625) {
-        double const y = -x, y2 = y * y, y4 = y2 * y2, y8 = y4 * y4;
-        double const a0 = fma(y, 1.0, 1.0), a1 = fma(y, 1.0 / 6.0, 0.5),
-                     a2 = fma(y, 1.0 / 120.0, 1.0 / 24.0), a3 = fma(y, 1.0 / 5040.0, 1.0 / 720.0),
-                     a4 = fma(y, 1.0 / 362880.0, 1.0 / 40320.0),
-                     a5 = fma(y, 1.0 / 39916800.0, 1.0 / 3628800.0);
-        expx = fma(y8, fma(y2, a5, a4), fma(y4, fma(y2, a3, a2), fma(y2, a1, a0)));
-        if (ax > 1e-3) {
-            double const b0 = fma(y, 0.5, 1.0), b1 = fma(y, 1.0 / 24.0, 1.0 / 6.0),
-                         b2 = fma(y, 1.0 / 720.0, 1.0 / 120.0),
-                         b3 = fma(y, 1.0 / 40320.0, 1.0 / 5040.0),
-                         b4 = fma(y, 1.0 / 3628800.0, 1.0 / 362880.0),
-                         b5 = fma(y, 1.0 / 479001600.0, 1.0 / 39916800.0);
-            op = fma(y8, fma(y2, b5, b4), fma(y4, fma(y2, b3, b2), fma(y2, b1, b0)));
-        } else {
-            double const c1 = -1.0 / 2.0, c2 = 1.0 / 6.0, c3 = -1.0 / 24.0, c4 = 1. / 120.,
-                         c5 = -1. / 720.;
-            op = 1.0 + x * (c1 + x * (c2 + x * (c3 + x * (c4 + x * c5))));
-        }
-        return;
-    }
+// exp(-x) and op(x) = (1 - exp(-x))/x of numerics.hpp:11-18.
+//
+// expx_exact is the reference's formula: the library exp, then op = (1 - e)/x, or for
+// |x| <= 1e-3 the reference's own 5th-order Taylor polynomial of op.
+//
+// expx_series evaluates both functions from their Taylor series, exp(-x) = sum (-x)^k/k!
+// and op(x) = sum (-x)^k/(k+1)!, to degree 11, by Estrin's scheme. For |x| <= 1/16 the
+// first omitted term is below 1e-23 relative, so both agree with the exact values to the
+// last bit or two (and op avoids the cancellation of 1 - e). It has no branch, so the
+// independent exponentials of a chain sweep can be interleaved; thermostat arguments are
+// x = dt p_eta/Q ~ dt/tau, far inside the series range. expx_operator takes the series
+// and falls back to expx_exact outside |x| <= 1/16.
+__device__ __forceinline__ void expx_exact(double x, double &expx, double &op) {
+    double const c1 = -1.0 / 2.0, c2 = 1.0 / 6.0, c3 = -1.0 / 24.0, c4 = 1. / 120.,
+                 c5 = -1. / 720.;
     double const e = exp(-x);
     expx = e;
-    op = (1.0 - e) / x;
+    op = fabs(x) > 1e-3 ? (1.0 - e) / x
+                        : 1.0 + x * (c1 + x * (c2 + x * (c3 + x * (c4 + x * c5))));
+}
+
+constexpr double kSeriesMax = 0.0625;
+
+__device__ __forceinline__ void expx_series(double x, double &expx, double &op) {
+    double const y = -x, y2 = y * y, y4 = y2 * y2, y8 = y4 * y4;
+    double const a0 = 1.0 + y, a1 = fma(y, 1.0 / 6.0, 0.5),
+                 a2 = fma(y, 1.0 / 120.0, 1.0 / 24.0), a3 = fma(y, 1.0 / 5040.0, 1.0 / 720.0),
+                 a4 = fma(y, 1.0 / 362880.0, 1.0 / 40320.0),
+                 a5 = fma(y, 1.0 / 39916800.0, 1.0 / 3628800.0);
+    expx = fma(y8, fma(y2, a5, a4), fma(y4, fma(y2, a3, a2), fma(y2, a1, a0)));
+    double const b0 = fma(y, 0.5, 1.0), b1 = fma(y, 1.0 / 24.0, 1.0 / 6.0),
+                 b2 = fma(y, 1.0 / 720.0, 1.0 / 120.0), b3 = fma(y, 1.0 / 40320.0, 1.0 / 5040.0),
+                 b4 = fma(y, 1.0 / 3628800.0, 1.0 / 362880.0),
+                 b5 = fma(y, 1.0 / 479001600.0, 1.0 / 39916800.0);
+    op = fma(y8, fma(y2, b5, b4), fma(y4, fma(y2, b3, b2), fma(y2, b1, b0)));
+}
+
+__device__ __forceinline__ void expx_operator(double x, double &expx, double &op) {
+    expx_series(x, expx, op);
+    if (fabs(x) > kSeriesMax)
+        expx_exact(x, expx, op);
 }
 
 __device__ __forceinline__ double volume(const double h[3]) { return h[0] * (h[1] * h[2]); }
@@ -106,10 +113,20 @@ template <int NC> __device__ __forceinline__ void U4_in(ChainR<NC> &c, double dt
 }
 
 template <int NC> __device__ __forceinline__ void U4_out(ChainR<NC> &c, double dt, double ec) {
-    double e[NC], op[NC];
+    double e[NC], op[NC], x[NC];
+    bool large = false;
 #pragma unroll
-    for (int j = 0; j < NC - 1; ++j)
-        expx_operator(dt * c.p[j + 1] * c.iq[j + 1], e[j], op[j]);
+    for (int j = 0; j < NC - 1; ++j) {
+        x[j] = dt * c.p[j + 1] * c.iq[j + 1];
+        expx_series(x[j], e[j], op[j]);
+        large |= fabs(x[j]) > kSeriesMax;
+    }
+    if (large) {
+#pragma unroll
+        for (int j = 0; j < NC - 1; ++j)
+            if (fabs(x[j]) > kSeriesMax)
+                expx_exact(x[j], e[j], op[j]);
+    }
 #pragma unroll
     for (int j = 0; j < NC; ++j) {
         double G;
