@@ -233,6 +233,28 @@ int mdelast_driver_get_chain(mdelast_driver *d, int32_t which, double *q, double
 int mdelast_driver_get_neighbors(mdelast_driver *d, int32_t *point, int32_t *neighbors,
                                  int64_t cap, int64_t *n_entries);
 
+/* ---------------------------------------------------------------------------------
+ * Batches: many independent replicas (cells of any size, composition, temperature,
+ * ensemble and seed) that share one potential, advanced together - every kernel of a
+ * step covers all replicas, and the scalar NHC/barostat work of the replicas runs side
+ * by side. The reference runs such replicas as separate processes
+ * (benchmarks/slurm_example.sh:6-24). A batch is a driver handle: mdelast_driver_run,
+ * _integrate, _calculate_neighbors, _set_sample_observables, _synchronize,
+ * _kernel_times and _destroy act on all its replicas; the readouts below take a replica
+ * index (the mdelast_driver_get_* functions read replica 0).
+ * ------------------------------------------------------------------------------- */
+/* cfgs[k] describes replica k; all must give the same pair/EAM handles and masses, the
+ * same neighbors, r_skin, precision and device. */
+int mdelast_batch_create(const mdelast_driver_config *cfgs, int32_t n_replicas,
+                         mdelast_driver **out);
+int mdelast_batch_size(const mdelast_driver *d, int32_t *n_replicas, int64_t *n_atoms);
+int mdelast_batch_get_observables(mdelast_driver *d, int32_t replica, mdelast_observables *out);
+int mdelast_batch_get_atoms(mdelast_driver *d, int32_t replica, int32_t field, double *out);
+int mdelast_batch_get_chain(mdelast_driver *d, int32_t replica, int32_t which, double *q,
+                            double *p_eta, double *eta, int32_t *nchain);
+int mdelast_batch_get_neighbors(mdelast_driver *d, int32_t replica, int32_t *point,
+                                int32_t *neighbors, int64_t cap, int64_t *n_entries);
+
 /* Pair correlation (md_driver.cpp:732-862): mode 0 calculate_pair_correlation,
  * 1 calculate_pair_correlations, 2 calculate_partial_pair_correlation. gr has n_rg
  * values, gr_partial n_types(n_types+1)/2 x n_rg. */

@@ -25,6 +25,7 @@ constexpr int kMaxChain = 16;
 constexpr int kTile = 256;  // replica atom ranges start on multiples of kTile slots
 constexpr int kBlock = 128; // threads per block of the atom kernels (divides kTile)
 constexpr int kMaxTypes = 8;
+constexpr int kChunk = 32;  // block sums folded per k_reduce block
 
 // Slots of the per-block partial sums of the force pass.
 enum FSlot : int {
@@ -115,6 +116,8 @@ struct AtomsView {
     int *nbr, *n_up, *n_dn;
     int maxn;
     double *pd, *pf; // per-block partial sums [n_blocks][D_NSUM], [n_blocks][F_NSUM]
+    double *red;     // chunk sums of pf/pd [n_rep][max_chunks][64] (k_reduce)
+    int max_chunks, pad_red;
     const int *dblk_rep, *fblk_rep; // replica of each block of the density / force pass
     // cell list (list builds)
     int *cell_count, *cell_atoms;

@@ -144,7 +144,12 @@ struct mdelast_driver_s {
             launch_force(obs, kick, tpa_f, grid_f, s, A, T);
     }
     int *d_nbr = nullptr, *d_nup = nullptr, *d_ndn = nullptr;
-    double *d_pd = nullptr, *d_pf = nullptr;
+    double *d_pd = nullptr, *d_pf = nullptr, *d_red = nullptr;
+    // closing scalar work: fold the block sums, then the per-replica kernel
+    void post(int mode, int obs, cudaStream_t s) {
+        k_reduce<<<dim3(A.max_chunks, n_rep), 256, 0, s>>>(A);
+        k_post<<<n_rep, 256, 0, s>>>(A, mode, obs);
+    }
     int *d_cell_count = nullptr, *d_cell_atoms = nullptr, *d_max_count = nullptr;
     double *d_rb = nullptr, *d_Ft = nullptr;
     double *d_pos0 = nullptr, *d_out = nullptr;
@@ -164,7 +169,10 @@ struct mdelast_driver_s {
     int alloc_cells(int n_cells, int cell_cap);
     void drop_graphs();
     int cells_alloc = 0;
-    int configure_cells(double const h[3]);
+    int configure_cells(std::vector<double> const &boxes); // 3 edges per replica
+    std::vector<double> current_boxes() const;
+    std::vector<int> rep_begin, rep_count; // atom slot range of each replica
+    std::vector<long> pos0_off;            // offset of each replica in d_pos0
     int enqueue_rebuild();
     int build_list_checked();
     int enqueue_step(int obs, int rebuild);
@@ -201,6 +209,7 @@ mdelast_driver_s::~mdelast_driver_s() {
     dfree(d_ndn);
     dfree(d_pd);
     dfree(d_pf);
+    dfree(d_red);
     dfree(d_cell_count);
     dfree(d_cell_atoms);
     dfree(d_max_count);
@@ -251,38 +260,53 @@ void mdelast_driver_s::drop_graphs() {
 // Cells per edge for the current box: no cell thinner than the list radius (with a margin
 // for the box changes of an NPT run between rebuilds); fewer than 3 along any edge means
 // an all-pairs search.
-int mdelast_driver_s::configure_cells(double const h[3]) {
-    int nc[3];
-    bool brute = false;
-    for (int a = 0; a < 3; ++a) {
-        nc[a] = static_cast<int>(std::floor(h[a] / (r_list * 1.05)));
-        if (nc[a] < 3)
-            brute = true;
-    }
-    if (brute)
-        nc[0] = nc[1] = nc[2] = 0;
-    int const n_cells = brute ? 0 : nc[0] * nc[1] * nc[2];
-    Replica r;
-    CK(cudaMemcpy(&r, d_rep, sizeof(Replica), cudaMemcpyDeviceToHost));
-    bool const changed = r.nc[0] != nc[0] || r.nc[1] != nc[1] || r.nc[2] != nc[2];
-    if (changed) {
+int mdelast_driver_s::configure_cells(std::vector<double> const &boxes) {
+    // per replica: cells per edge from its box, and its block of the global cell arrays
+    std::vector<Replica> R(static_cast<size_t>(n_rep));
+    CK(cudaMemcpy(R.data(), d_rep, sizeof(Replica) * n_rep, cudaMemcpyDeviceToHost));
+    bool changed = false, all_brute = true;
+    int n_cells = 0, cap = std::max(A.cell_cap, 64);
+    for (int q = 0; q < n_rep; ++q) {
+        int nc[3];
+        bool brute = false;
+        for (int a = 0; a < 3; ++a) {
+            nc[a] = static_cast<int>(std::floor(boxes[3 * q + a] / (r_list * 1.05)));
+            if (nc[a] < 3)
+                brute = true;
+        }
+        if (brute)
+            nc[0] = nc[1] = nc[2] = 0;
+        Replica &r = R[static_cast<size_t>(q)];
+        if (r.nc[0] != nc[0] || r.nc[1] != nc[1] || r.nc[2] != nc[2] || r.cell_begin != n_cells)
+            changed = true;
         r.nc[0] = nc[0];
         r.nc[1] = nc[1];
         r.nc[2] = nc[2];
-        r.cell_begin = 0;
-        CK(cudaMemcpy(d_rep, &r, sizeof(Replica), cudaMemcpyHostToDevice));
+        r.cell_begin = n_cells;
+        int const nq = brute ? 0 : nc[0] * nc[1] * nc[2];
+        if (nq > 0)
+            cap = std::max(cap, static_cast<int>(2. * r.n_atoms / nq) + 64);
+        n_cells += nq;
+        all_brute = all_brute && brute;
     }
-    int cap = std::max(A.cell_cap, 64);
-    if (n_cells > 0)
-        cap = std::max(cap, static_cast<int>(2. * N / n_cells) + 64);
+    if (changed)
+        CK(cudaMemcpy(d_rep, R.data(), sizeof(Replica) * n_rep, cudaMemcpyHostToDevice));
     if (!d_cell_count || n_cells > cells_alloc || cap > A.cell_cap)
         if (int rc = alloc_cells(std::max(n_cells, cells_alloc), cap))
             return rc;
-    if (changed || all_pairs != brute || A.n_cells != n_cells)
+    if (changed || all_pairs != all_brute || A.n_cells != n_cells)
         drop_graphs(); // the launch shape of the cell kernels is part of the graphs
-    all_pairs = brute;
+    all_pairs = all_brute;
     A.n_cells = n_cells;
     return MDELAST_OK;
+}
+
+std::vector<double> mdelast_driver_s::current_boxes() const {
+    std::vector<double> b;
+    for (int q = 0; q < n_rep; ++q)
+        for (int a = 0; a < 3; ++a)
+            b.push_back(h_obs[q].box[4 * a]);
+    return b;
 }
 
 int mdelast_driver_s::enqueue_rebuild() {
@@ -339,7 +363,7 @@ int mdelast_driver_s::enqueue_step(int obs, int rebuild) {
             return rc;
     pass_density(obs != 0, stream);
     pass_force(obs != 0, true, stream);
-    k_post<<<n_rep, 256, 0, stream>>>(A, POST_STEP, obs);
+    post(POST_STEP, obs, stream);
     CK(cudaGetLastError());
     CK(cudaMemcpy2DAsync(h_obs, sizeof(mdelast_observables),
                          reinterpret_cast<char *>(d_rep) + offsetof(Replica, obs), sizeof(Replica),
@@ -423,17 +447,16 @@ int mdelast_device_available(void) {
     return n > 0;
 }
 
-int mdelast_driver_create(const mdelast_driver_config *cfg, mdelast_driver **out) {
-    clear_error();
-    if (!cfg || !out)
-        return fail(MDELAST_ERR_ARGUMENT, "null argument");
-    *out = nullptr;
-    mdelast_driver_config const &c = *cfg;
+} // extern "C"
+
+// Validate one replica's configuration against the shared tables (those of replica 0).
+static int check_config(mdelast_driver_config const &c, mdelast_driver_config const &c0, int r) {
     int const N = c.n_atoms, nt = c.n_types;
     if (N < 2 || nt < 1 || nt > kMaxTypes)
-        return fail(MDELAST_ERR_ARGUMENT, "need n_atoms >= 2 and 1 <= n_types <= %d", kMaxTypes);
+        return fail(MDELAST_ERR_ARGUMENT, "replica %d: need n_atoms >= 2 and 1 <= n_types <= %d",
+                    r, kMaxTypes);
     if (!c.positions || !c.velocities || !c.types || !c.mass || !c.pair)
-        return fail(MDELAST_ERR_ARGUMENT, "null array in the driver configuration");
+        return fail(MDELAST_ERR_ARGUMENT, "replica %d: null array in the configuration", r);
     int const npot = nt * (nt + 1) / 2;
     if (c.n_eam != 0 && c.n_eam != nt)
         return fail(MDELAST_ERR_ARGUMENT, "EAM objects: %d given, %d types", c.n_eam, nt);
@@ -476,31 +499,95 @@ int mdelast_driver_create(const mdelast_driver_config *cfg, mdelast_driver **out
             e->F.n != c.eam[0]->F.n || e->F.h != c.eam[0]->F.h)
             return fail(MDELAST_ERR_UNSUPPORTED, "EAM tables on different grids");
     }
-    double const L[3] = {c.box[0], c.box[4], c.box[8]};
-    std::vector<double4> crd(static_cast<size_t>(N));
-    for (int i = 0; i < N; ++i) {
-        double const *p = c.positions + 3 * i;
-        // md_driver.cpp:91-106
-        if (std::abs(p[0]) >= 0.5 * L[0] || std::abs(p[1]) >= 0.5 * L[1] ||
-            std::abs(p[2]) >= 0.5 * L[2])
-            return fail(MDELAST_ERR_ARGUMENT, "bad initial position (atom %d)", i);
-        if (c.types[i] >= static_cast<uint32_t>(nt))
-            return fail(MDELAST_ERR_ARGUMENT, "bad type (atom %d)", i);
-        double u[3] = {p[0] / L[0], p[1] / L[1], p[2] / L[2]};
-        crd[i] = make_double4(u[0] - nint_host(u[0]), u[1] - nint_host(u[1]),
-                              u[2] - nint_host(u[2]), static_cast<double>(c.types[i]));
+    if (r > 0) { // a batch shares the tables, the list settings, the precision and the device
+        bool same = c.n_types == c0.n_types && c.n_eam == c0.n_eam &&
+                    c.neighbors == c0.neighbors && c.r_skin == c0.r_skin &&
+                    c.precision == c0.precision && c.device == c0.device;
+        for (int s = 0; same && s < npot; ++s)
+            same = c.pair[s] == c0.pair[s];
+        for (int t = 0; same && t < c.n_eam; ++t)
+            same = c.eam[t] == c0.eam[t];
+        for (int t = 0; same && t < nt; ++t)
+            same = c.mass[t] == c0.mass[t];
+        if (!same)
+            return fail(MDELAST_ERR_ARGUMENT,
+                        "replica %d: a batch shares potentials, masses, list settings, "
+                        "precision and device with replica 0", r);
+    }
+    return MDELAST_OK;
+}
+
+static void set_chain(Chain &ch, double T_, int n, const double *q, const double *p, double Nf) {
+    ch.T = T_;
+    ch.Nf = Nf;
+    ch.n = n;
+    for (int j = 0; j < n; ++j) {
+        ch.q[j] = q[j];
+        ch.inv_q[j] = 1. / q[j];
+        ch.p_eta[j] = p[j];
+        ch.eta[j] = 0.;
+    }
+}
+
+// A system of n_rep independent replicas sharing one potential (n_rep = 1: MDDriver).
+static int create_system(const mdelast_driver_config *cfgs, int n_rep, mdelast_driver **out) {
+    clear_error();
+    if (!cfgs || !out || n_rep < 1)
+        return fail(MDELAST_ERR_ARGUMENT, "null argument or no replica");
+    *out = nullptr;
+    mdelast_driver_config const &c0 = cfgs[0];
+    for (int r = 0; r < n_rep; ++r)
+        if (int rc = check_config(cfgs[r], c0, r))
+            return rc;
+    int const nt = c0.n_types, npot = nt * (nt + 1) / 2;
+    // scaled coordinates (md_driver.cpp:91-106) of every replica, packed at kTile offsets
+    std::vector<int> begin(static_cast<size_t>(n_rep)), count(static_cast<size_t>(n_rep));
+    int np = 0;
+    long n_total = 0;
+    for (int r = 0; r < n_rep; ++r) {
+        begin[r] = np;
+        count[r] = cfgs[r].n_atoms;
+        np += (cfgs[r].n_atoms + kTile - 1) / kTile * kTile;
+        n_total += cfgs[r].n_atoms;
+    }
+    std::vector<double4> crd(static_cast<size_t>(np), make_double4(0, 0, 0, 0));
+    std::vector<int> rep_of(static_cast<size_t>(np), -1);
+    std::vector<double> vel(3 * static_cast<size_t>(np), 0.);
+    std::vector<double> pos0(3 * static_cast<size_t>(n_total));
+    long p0off = 0;
+    for (int r = 0; r < n_rep; ++r) {
+        mdelast_driver_config const &c = cfgs[r];
+        double const L[3] = {c.box[0], c.box[4], c.box[8]};
+        for (int a = 0; a < c.n_atoms; ++a) {
+            double const *p = c.positions + 3 * a;
+            if (std::abs(p[0]) >= 0.5 * L[0] || std::abs(p[1]) >= 0.5 * L[1] ||
+                std::abs(p[2]) >= 0.5 * L[2])
+                return fail(MDELAST_ERR_ARGUMENT, "bad initial position (replica %d atom %d)", r, a);
+            if (c.types[a] >= static_cast<uint32_t>(nt))
+                return fail(MDELAST_ERR_ARGUMENT, "bad type (replica %d atom %d)", r, a);
+            double const u[3] = {p[0] / L[0], p[1] / L[1], p[2] / L[2]};
+            size_t const i = static_cast<size_t>(begin[r] + a);
+            crd[i] = make_double4(u[0] - nint_host(u[0]), u[1] - nint_host(u[1]),
+                                  u[2] - nint_host(u[2]), static_cast<double>(c.types[a]));
+            rep_of[i] = r;
+            for (int k = 0; k < 3; ++k) {
+                vel[static_cast<size_t>(k) * np + i] = c.velocities[3 * a + k];
+                pos0[static_cast<size_t>(p0off + 3 * a + k)] = p[k];
+            }
+        }
+        p0off += 3L * c.n_atoms;
     }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
         return fail(MDELAST_ERR_NO_DEVICE, "no CUDA device: the mdelast GPU path needs one");
     }
-    if (c.device < 0 || c.device >= ndev)
-        return fail(MDELAST_ERR_ARGUMENT, "device %d not present (%d devices)", c.device, ndev);
-    CK(cudaSetDevice(c.device));
+    if (c0.device < 0 || c0.device >= ndev)
+        return fail(MDELAST_ERR_ARGUMENT, "device %d not present (%d devices)", c0.device, ndev);
+    CK(cudaSetDevice(c0.device));
 
     auto *d = new mdelast_driver_s();
-    d->device = c.device;
+    d->device = c0.device;
     auto bail = [&](int rc) {
         delete d;
         return rc;
@@ -513,16 +600,19 @@ int mdelast_driver_create(const mdelast_driver_config *cfg, mdelast_driver **out
     } while (0)
     if (cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) != cudaSuccess)
         return bail(fail(MDELAST_ERR_CUDA, "stream creation failed"));
-    d->N = N;
+    d->n_rep = n_rep;
+    d->rep_begin = begin;
+    d->rep_count = count;
+    d->N = static_cast<int>(n_total);
     d->ntypes = nt;
     d->npot = npot;
-    d->n_pad = (N + kTile - 1) / kTile * kTile;
-    d->n_blocks = d->n_pad / kBlock;
-    d->neighbors = c.neighbors != 0;
-    d->r_skin = c.r_skin;
+    d->n_pad = np;
+    d->n_blocks = np / kBlock;
+    d->neighbors = c0.neighbors != 0;
+    d->r_skin = c0.r_skin;
+    mdelast_pair const *p0 = c0.pair[0];
     double const rcut = p0->rcut;
-    d->r_list = d->neighbors ? rcut * c.r_skin : rcut;
-    int const np = d->n_pad;
+    d->r_list = d->neighbors ? rcut * c0.r_skin : rcut;
 
     // ---- tables: r-table bundles and embedding tables
     int const nri = p0->table.n;
@@ -532,20 +622,20 @@ int mdelast_driver_create(const mdelast_driver_config *cfg, mdelast_driver **out
             int const s = b * (b + 1) / 2 + a;
             for (int k = 0; k < nri; ++k) {
                 double *o = rb.data() + (static_cast<size_t>(s) * nri + k) * 18;
-                std::memcpy(o, c.pair[s]->table.coef.data() + 6 * static_cast<size_t>(k),
+                std::memcpy(o, c0.pair[s]->table.coef.data() + 6 * static_cast<size_t>(k),
                             6 * sizeof(double));
-                if (c.n_eam) {
-                    std::memcpy(o + 6, c.eam[a]->rho.coef.data() + 6 * static_cast<size_t>(k),
+                if (c0.n_eam) {
+                    std::memcpy(o + 6, c0.eam[a]->rho.coef.data() + 6 * static_cast<size_t>(k),
                                 6 * sizeof(double));
-                    std::memcpy(o + 12, c.eam[b]->rho.coef.data() + 6 * static_cast<size_t>(k),
+                    std::memcpy(o + 12, c0.eam[b]->rho.coef.data() + 6 * static_cast<size_t>(k),
                                 6 * sizeof(double));
                 }
             }
         }
-    int const nfi = c.n_eam ? c.eam[0]->F.n : 1;
+    int const nfi = c0.n_eam ? c0.eam[0]->F.n : 1;
     std::vector<double> Ft(static_cast<size_t>(nt) * nfi * 6, 0.);
-    for (int t = 0; t < c.n_eam; ++t)
-        std::memcpy(Ft.data() + static_cast<size_t>(t) * nfi * 6, c.eam[t]->F.coef.data(),
+    for (int t = 0; t < c0.n_eam; ++t)
+        std::memcpy(Ft.data() + static_cast<size_t>(t) * nfi * 6, c0.eam[t]->F.coef.data(),
                     sizeof(double) * 6 * nfi);
     TRY(dalloc(&d->d_rb, rb.size()));
     TRY(dalloc(&d->d_Ft, Ft.size()));
@@ -561,21 +651,21 @@ int mdelast_driver_create(const mdelast_driver_config *cfg, mdelast_driver **out
     T.Ft = d->d_Ft;
     T.nfi = nfi;
     T.ntypes = nt;
-    T.inv_hf = c.n_eam ? c.eam[0]->F.inv_h : 1.;
-    T.inv_hf2 = c.n_eam ? c.eam[0]->F.inv_h2 : 1.;
-    T.has_eam = c.n_eam > 0;
+    T.inv_hf = c0.n_eam ? c0.eam[0]->F.inv_h : 1.;
+    T.inv_hf2 = c0.n_eam ? c0.eam[0]->F.inv_h2 : 1.;
+    T.has_eam = c0.n_eam > 0;
     T.r_cut_sq = rcut * rcut;
     for (int s = 0; s < npot; ++s) {
-        T.pot_rcut[s] = c.pair[s]->rcut;
-        T.pot_rmin[s] = c.pair[s]->rmin_fatal;
+        T.pot_rcut[s] = c0.pair[s]->rcut;
+        T.pot_rmin[s] = c0.pair[s]->rmin_fatal;
     }
     for (int t = 0; t < nt; ++t) {
-        T.eam_rcut[t] = c.n_eam ? c.eam[t]->rcut : 0.;
-        T.rhomax[t] = c.n_eam ? c.eam[t]->rhomax_fatal : 0.;
-        T.mass[t] = c.mass[t];
+        T.eam_rcut[t] = c0.n_eam ? c0.eam[t]->rcut : 0.;
+        T.rhomax[t] = c0.n_eam ? c0.eam[t]->rhomax_fatal : 0.;
+        T.mass[t] = c0.mass[t];
     }
-    d->precision = c.precision;
-    if (c.precision == MDELAST_PRECISION_MIXED) {
+    d->precision = c0.precision;
+    if (c0.precision == MDELAST_PRECISION_MIXED) {
         // the r bundles in FP32, angstrom / eV (phi) and angstrom^-3 (rho)
         std::vector<float> rbf(rb.size());
         double const a3 = kAng * kAng * kAng;
@@ -596,64 +686,48 @@ int mdelast_driver_create(const mdelast_driver_config *cfg, mdelast_driver **out
             T.feam_rcut[t] = static_cast<float>(T.eam_rcut[t] / kAng);
     }
 
-    // ---- replica state
-    Replica R;
-    std::memset(&R, 0, sizeof(R));
-    R.atom_begin = 0;
-    R.n_atoms = N;
-    R.block_begin = 0;
-    R.n_blocks = d->n_blocks;
-    R.ensemble = c.ensemble;
-    R.coupling = c.coupling;
-    R.Nf = c.Nf;
-    R.alpha = 1. + 3. / c.Nf;
-    R.dt = c.dt;
-    R.fatal_conservation = c.fatal_conservation;
-    R.mass0 = c.mass[0];
-    R.baro_P = c.baro_P;
-    R.baro_w = c.baro_w;
-    for (int a = 0; a < 3; ++a)
-        R.h0[a] = R.h[a] = R.h_pos[a] = L[a];
-    R.eps = 0.;
-    R.p_eps = c.baro_p_eps;
-    R.vscale = 1.;
-    auto set_chain = [](Chain &ch, double T_, int n, const double *q, const double *p,
-                        double Nf) {
-        ch.T = T_;
-        ch.Nf = Nf;
-        ch.n = n;
-        for (int j = 0; j < n; ++j) {
-            ch.q[j] = q[j];
-            ch.inv_q[j] = 1. / q[j];
-            ch.p_eta[j] = p[j];
-            ch.eta[j] = 0.;
-        }
-    };
-    set_chain(R.th, c.thermo_T, c.thermo_nchain, c.thermo_q, c.thermo_p_eta, c.thermo_Nf);
-    set_chain(R.bth, c.baro_thermo_T, c.baro_nchain, c.baro_q, c.baro_p_eta, c.baro_Nf);
-
-    d->tpa_d = d->tpa_f = default_tpa(N);
-    std::vector<Replica *> reps{&R};
+    // ---- replica states
+    std::vector<Replica> R(static_cast<size_t>(n_rep));
+    std::vector<Replica *> reps;
+    for (int r = 0; r < n_rep; ++r) {
+        mdelast_driver_config const &c = cfgs[r];
+        Replica &x = R[static_cast<size_t>(r)];
+        std::memset(&x, 0, sizeof(Replica));
+        x.atom_begin = begin[r];
+        x.n_atoms = c.n_atoms;
+        x.block_begin = begin[r] / kBlock;
+        x.n_blocks = (c.n_atoms + kTile - 1) / kTile * kTile / kBlock;
+        x.ensemble = c.ensemble;
+        x.coupling = c.coupling;
+        x.Nf = c.Nf;
+        x.alpha = 1. + 3. / c.Nf;
+        x.dt = c.dt;
+        x.fatal_conservation = c.fatal_conservation;
+        x.mass0 = c.mass[0];
+        x.baro_P = c.baro_P;
+        x.baro_w = c.baro_w;
+        for (int a = 0; a < 3; ++a)
+            x.h0[a] = x.h[a] = x.h_pos[a] = c.box[4 * a];
+        x.eps = 0.;
+        x.p_eps = c.baro_p_eps;
+        x.vscale = 1.;
+        set_chain(x.th, c.thermo_T, c.thermo_nchain, c.thermo_q, c.thermo_p_eta, c.thermo_Nf);
+        set_chain(x.bth, c.baro_thermo_T, c.baro_nchain, c.baro_q, c.baro_p_eta, c.baro_Nf);
+        reps.push_back(&x);
+    }
+    d->tpa_d = d->tpa_f = default_tpa(static_cast<int>(std::min<long>(n_total, 1L << 30)));
     std::vector<int> dmap, fmap;
     d->grid_d = deal_blocks(reps, d->tpa_d, true, dmap);
     d->grid_f = deal_blocks(reps, d->tpa_f, false, fmap);
     TRY(dalloc(&d->d_dblk_rep, dmap.size()));
     TRY(dalloc(&d->d_fblk_rep, fmap.size()));
-    TRY(dalloc(&d->d_rep, 1));
-    if (cudaMemcpy(d->d_rep, &R, sizeof(R), cudaMemcpyHostToDevice) ||
+    TRY(dalloc(&d->d_rep, static_cast<size_t>(n_rep)));
+    if (cudaMemcpy(d->d_rep, R.data(), sizeof(Replica) * n_rep, cudaMemcpyHostToDevice) ||
         cudaMemcpy(d->d_dblk_rep, dmap.data(), sizeof(int) * dmap.size(), cudaMemcpyHostToDevice) ||
         cudaMemcpy(d->d_fblk_rep, fmap.data(), sizeof(int) * fmap.size(), cudaMemcpyHostToDevice))
         return bail(fail(MDELAST_ERR_CUDA, "state upload failed"));
 
     // ---- atoms
-    std::vector<int> rep_of(static_cast<size_t>(np), -1);
-    std::fill(rep_of.begin(), rep_of.begin() + N, 0);
-    std::vector<double4> crd_pad(static_cast<size_t>(np), make_double4(0, 0, 0, 0));
-    std::copy(crd.begin(), crd.end(), crd_pad.begin());
-    std::vector<double> vel(3 * static_cast<size_t>(np), 0.);
-    for (int i = 0; i < N; ++i)
-        for (int a = 0; a < 3; ++a)
-            vel[static_cast<size_t>(a) * np + i] = c.velocities[3 * i + a];
     TRY(dalloc(&d->d_rep_of, np));
     TRY(dalloc(&d->d_crd, np));
     TRY(dalloc(&d->d_vel, 3 * static_cast<size_t>(np)));
@@ -662,7 +736,7 @@ int mdelast_driver_create(const mdelast_driver_config *cfg, mdelast_driver **out
     TRY(dalloc(&d->d_Fe, np));
     TRY(dalloc(&d->d_epot, np));
     TRY(dalloc(&d->d_dF2, np));
-    if (c.precision == MDELAST_PRECISION_MIXED) {
+    if (c0.precision == MDELAST_PRECISION_MIXED) {
         TRY(dalloc(&d->d_posf, np));
         TRY(dalloc(&d->d_dF2f, np));
     }
@@ -670,21 +744,31 @@ int mdelast_driver_create(const mdelast_driver_config *cfg, mdelast_driver **out
     TRY(dalloc(&d->d_ndn, np));
     TRY(dalloc(&d->d_pd, static_cast<size_t>(d->grid_d) * D_NSUM));
     TRY(dalloc(&d->d_pf, static_cast<size_t>(d->grid_f) * F_NSUM));
+    int max_chunks = 1;
+    for (Replica const *x : reps)
+        max_chunks = std::max(max_chunks, (std::max(x->dblk_n, x->fblk_n) + kChunk - 1) / kChunk);
+    TRY(dalloc(&d->d_red, static_cast<size_t>(n_rep) * max_chunks * 64));
     TRY(dalloc(&d->d_max_count, 2));
-    TRY(dalloc(&d->d_pos0, 3 * static_cast<size_t>(N)));
-    TRY(dalloc(&d->d_out, 3 * static_cast<size_t>(N)));
+    TRY(dalloc(&d->d_pos0, pos0.size()));
+    int max_n = 0;
+    for (int r = 0; r < n_rep; ++r)
+        max_n = std::max(max_n, count[r]);
+    TRY(dalloc(&d->d_out, 3 * static_cast<size_t>(max_n)));
+    d->pos0_off.assign(static_cast<size_t>(n_rep), 0);
+    for (int r = 1; r < n_rep; ++r)
+        d->pos0_off[r] = d->pos0_off[r - 1] + 3L * count[r - 1];
     if (cudaMemcpy(d->d_rep_of, rep_of.data(), sizeof(int) * np, cudaMemcpyHostToDevice) ||
-        cudaMemcpy(d->d_crd, crd_pad.data(), sizeof(double4) * np, cudaMemcpyHostToDevice) ||
+        cudaMemcpy(d->d_crd, crd.data(), sizeof(double4) * np, cudaMemcpyHostToDevice) ||
         cudaMemcpy(d->d_vel, vel.data(), sizeof(double) * vel.size(), cudaMemcpyHostToDevice) ||
-        cudaMemcpy(d->d_pos0, c.positions, sizeof(double) * 3 * N, cudaMemcpyHostToDevice))
+        cudaMemcpy(d->d_pos0, pos0.data(), sizeof(double) * pos0.size(), cudaMemcpyHostToDevice))
         return bail(fail(MDELAST_ERR_CUDA, "atom upload failed"));
-    if (cudaMallocHost(&d->h_obs, sizeof(mdelast_observables) * d->n_rep) ||
+    if (cudaMallocHost(&d->h_obs, sizeof(mdelast_observables) * n_rep) ||
         cudaEventCreateWithFlags(&d->ev_step, cudaEventDisableTiming))
         return bail(fail(MDELAST_ERR_CUDA, "host staging allocation failed"));
 
     AtomsView &A = d->A;
     A.n_pad = np;
-    A.n_rep = d->n_rep;
+    A.n_rep = n_rep;
     A.rep = d->d_rep;
     A.rep_of = d->d_rep_of;
     A.crd = d->d_crd;
@@ -700,22 +784,32 @@ int mdelast_driver_create(const mdelast_driver_config *cfg, mdelast_driver **out
     A.n_dn = d->d_ndn;
     A.pd = d->d_pd;
     A.pf = d->d_pf;
+    A.red = d->d_red;
+    A.max_chunks = max_chunks;
     A.dblk_rep = d->d_dblk_rep;
     A.fblk_rep = d->d_fblk_rep;
     A.max_count = d->d_max_count;
-    A.r_list_sq = d->r_list * d->r_list;
     if (d->neighbors) // md_driver.cpp:42: pow<2>(pot[0]->rcut * r_skin)
-        A.r_list_sq = (rcut * c.r_skin) * (rcut * c.r_skin);
+        A.r_list_sq = (rcut * c0.r_skin) * (rcut * c0.r_skin);
     else
         A.r_list_sq = rcut * rcut;
 
-    // neighbour capacity from the number density: 1.5 x the mean count + 32
-    double const vol = L[0] * (L[1] * L[2]);
-    double const mean = 4. / 3. * M_PI * std::pow(d->r_list, 3) * N / vol;
-    int maxn = static_cast<int>(1.5 * std::min(mean, static_cast<double>(N))) + 32;
-    maxn = std::min((maxn + 3) / 4 * 4, (N + 3) / 4 * 4);
-    TRY(d->alloc_list(std::max(maxn, 4)));
-    TRY(d->configure_cells(L));
+    // neighbour capacity from the densest replica: 1.5 x its mean count + 32
+    int maxn = 4;
+    for (int r = 0; r < n_rep; ++r) {
+        mdelast_driver_config const &c = cfgs[r];
+        double const vol = c.box[0] * (c.box[4] * c.box[8]);
+        double const mean = 4. / 3. * M_PI * std::pow(d->r_list, 3) * c.n_atoms / vol;
+        int m = static_cast<int>(1.5 * std::min(mean, static_cast<double>(c.n_atoms))) + 32;
+        m = std::min((m + 3) / 4 * 4, (c.n_atoms + 3) / 4 * 4);
+        maxn = std::max(maxn, m);
+    }
+    TRY(d->alloc_list(maxn));
+    std::vector<double> boxes;
+    for (int r = 0; r < n_rep; ++r)
+        for (int a = 0; a < 3; ++a)
+            boxes.push_back(cfgs[r].box[4 * a]);
+    TRY(d->configure_cells(boxes));
 
     // ---- the constructor's force call and thermodynamics (md_driver.cpp:112-118)
     TRY(d->build_list_checked());
@@ -723,7 +817,7 @@ int mdelast_driver_create(const mdelast_driver_config *cfg, mdelast_driver **out
         k_posf<<<np / kBlock, kBlock, 0, d->stream>>>(d->A);
     d->pass_density(true, d->stream);
     d->pass_force(true, false, d->stream);
-    k_post<<<d->n_rep, 256, 0, d->stream>>>(d->A, POST_INIT, 1);
+    d->post(POST_INIT, 1, d->stream);
     if (cudaGetLastError() != cudaSuccess)
         return bail(fail(MDELAST_ERR_CUDA, "kernel launch failed"));
     if (cudaMemcpy2DAsync(d->h_obs, sizeof(mdelast_observables),
@@ -738,6 +832,12 @@ int mdelast_driver_create(const mdelast_driver_config *cfg, mdelast_driver **out
 #undef TRY
     *out = d;
     return MDELAST_OK;
+}
+
+extern "C" {
+
+int mdelast_driver_create(const mdelast_driver_config *cfg, mdelast_driver **out) {
+    return create_system(cfg, 1, out);
 }
 
 void mdelast_driver_destroy(mdelast_driver *d) { delete d; }
@@ -761,8 +861,7 @@ int mdelast_driver_run(mdelast_driver *d, int32_t n_steps, int32_t rebuild_every
     if (int rc = d->wait_step())
         return rc;
     if (d->neighbors && rebuild_every > 0) { // cell geometry for the current box
-        double h[3] = {d->h_obs[0].box[0], d->h_obs[0].box[4], d->h_obs[0].box[8]};
-        if (int rc = d->configure_cells(h))
+        if (int rc = d->configure_cells(d->current_boxes()))
             return rc;
     }
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -814,7 +913,7 @@ int mdelast_driver_kernel_times(mdelast_driver *d, int32_t n_steps, double *ms_o
         cudaEventRecord(ev[4], s);
         d->pass_force(true, true, s);
         cudaEventRecord(ev[5], s);
-        k_post<<<d->n_rep, 256, 0, s>>>(d->A, POST_STEP, 1);
+        d->post(POST_STEP, 1, s);
         cudaEventRecord(ev[6], s);
         cudaError_t e = cudaEventSynchronize(ev[6]);
         if (e != cudaSuccess) {
@@ -853,8 +952,7 @@ int mdelast_driver_calculate_neighbors(mdelast_driver *d) {
     if (!d->neighbors) // the reference writes into empty point/neighbors storage
         return fail(MDELAST_ERR_UNSUPPORTED,
                     "calculate_neighbors() needs a driver created with neighbors=True");
-    double h[3] = {d->h_obs[0].box[0], d->h_obs[0].box[4], d->h_obs[0].box[8]};
-    if (int rc = d->configure_cells(h))
+    if (int rc = d->configure_cells(d->current_boxes()))
         return rc;
     return d->build_list_checked();
 }
@@ -882,25 +980,29 @@ int mdelast_driver_synchronize(mdelast_driver *d) {
     return d->wait_step();
 }
 
-int mdelast_driver_get_observables(mdelast_driver *d, mdelast_observables *out) {
+} // extern "C"
+
+// Readouts of replica r (r = 0 for a single driver).
+static int get_observables_r(mdelast_driver *d, int r, mdelast_observables *out) {
     clear_error();
-    if (!d || !out)
-        return fail(MDELAST_ERR_ARGUMENT, "null argument");
+    if (!d || !out || r < 0 || r >= d->n_rep)
+        return fail(MDELAST_ERR_ARGUMENT, "bad argument");
     CK(cudaSetDevice(d->device));
     int const rc = d->wait_step();
-    *out = d->h_obs[0];
+    *out = d->h_obs[r];
     return rc;
 }
 
-int mdelast_driver_get_atoms(mdelast_driver *d, int32_t field, double *out) {
+static int get_atoms_r(mdelast_driver *d, int r, int32_t field, double *out) {
     clear_error();
-    if (!d || !out || field < 0 || field > MDELAST_ATOM_EKIN)
+    if (!d || !out || field < 0 || field > MDELAST_ATOM_EKIN || r < 0 || r >= d->n_rep)
         return fail(MDELAST_ERR_ARGUMENT, "bad argument");
     CK(cudaSetDevice(d->device));
     if (int rc = d->wait_step())
         return rc;
-    int const N = d->N;
-    k_readout<<<(N + 255) / 256, 256, 0, d->stream>>>(d->A, d->T, 0, field, d->d_out, d->d_pos0,
+    int const N = d->rep_count[r];
+    k_readout<<<(N + 255) / 256, 256, 0, d->stream>>>(d->A, d->T, r, field, d->d_out,
+                                                      d->d_pos0 + d->pos0_off[r],
                                                       d->stepped ? 1 : 0);
     CK(cudaGetLastError());
     size_t const n = field <= MDELAST_ATOM_FORCES ? 3 * static_cast<size_t>(N) : N;
@@ -909,16 +1011,17 @@ int mdelast_driver_get_atoms(mdelast_driver *d, int32_t field, double *out) {
     return MDELAST_OK;
 }
 
-int mdelast_driver_get_chain(mdelast_driver *d, int32_t which, double *q, double *p_eta,
-                             double *eta, int32_t *nchain) {
+static int get_chain_r(mdelast_driver *d, int r, int32_t which, double *q, double *p_eta,
+                       double *eta, int32_t *nchain) {
     clear_error();
-    if (!d || (which != 0 && which != 1))
+    if (!d || (which != 0 && which != 1) || r < 0 || r >= d->n_rep)
         return fail(MDELAST_ERR_ARGUMENT, "bad argument");
     CK(cudaSetDevice(d->device));
     if (int rc = d->wait_step())
         return rc;
     Chain ch;
-    size_t const off = which == 0 ? offsetof(Replica, th) : offsetof(Replica, bth);
+    size_t const off = static_cast<size_t>(r) * sizeof(Replica) +
+                       (which == 0 ? offsetof(Replica, th) : offsetof(Replica, bth));
     CK(cudaMemcpy(&ch, reinterpret_cast<char *>(d->d_rep) + off, sizeof(Chain),
                   cudaMemcpyDeviceToHost));
     for (int j = 0; j < ch.n; ++j) {
@@ -934,24 +1037,24 @@ int mdelast_driver_get_chain(mdelast_driver *d, int32_t which, double *q, double
     return MDELAST_OK;
 }
 
-int mdelast_driver_get_neighbors(mdelast_driver *d, int32_t *point, int32_t *neighbors,
-                                 int64_t cap, int64_t *n_entries) {
+static int get_neighbors_r(mdelast_driver *d, int r, int32_t *point, int32_t *neighbors,
+                           int64_t cap, int64_t *n_entries) {
     clear_error();
-    if (!d || !point)
-        return fail(MDELAST_ERR_ARGUMENT, "null argument");
+    if (!d || !point || r < 0 || r >= d->n_rep)
+        return fail(MDELAST_ERR_ARGUMENT, "bad argument");
     if (!d->neighbors)
         return fail(MDELAST_ERR_UNSUPPORTED, "neighbour lists are disabled for this driver");
     CK(cudaSetDevice(d->device));
     if (int rc = d->wait_step())
         return rc;
-    int const N = d->N;
+    int const N = d->rep_count[r];
     if (d->tmp_i_cap < static_cast<size_t>(N) + 1) {
         dfree(d->d_tmp_i);
         if (int rc = dalloc(&d->d_tmp_i, static_cast<size_t>(N) + 1))
             return rc;
         d->tmp_i_cap = static_cast<size_t>(N) + 1;
     }
-    k_half_list_counts<<<(N + 255) / 256, 256, 0, d->stream>>>(d->A, 0, d->d_tmp_i);
+    k_half_list_counts<<<(N + 255) / 256, 256, 0, d->stream>>>(d->A, r, d->d_tmp_i);
     std::vector<int> cnt(static_cast<size_t>(N));
     CK(cudaMemcpyAsync(cnt.data(), d->d_tmp_i, sizeof(int) * N, cudaMemcpyDeviceToHost,
                        d->stream));
@@ -973,11 +1076,13 @@ int mdelast_driver_get_neighbors(mdelast_driver *d, int32_t *point, int32_t *nei
         dfree(d_point);
         return rc;
     }
-    cudaMemcpy(d_point, point, sizeof(int) * (N + 1), cudaMemcpyHostToDevice);
-    k_half_list_fill<<<(N + 255) / 256, 256, 0, d->stream>>>(d->A, 0, d_point, d_list);
-    cudaError_t e = cudaMemcpyAsync(neighbors, d_list,
-                                    sizeof(int) * static_cast<size_t>(std::min(total, cap)),
-                                    cudaMemcpyDeviceToHost, d->stream);
+    cudaError_t e = cudaMemcpy(d_point, point, sizeof(int) * (N + 1), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        k_half_list_fill<<<(N + 255) / 256, 256, 0, d->stream>>>(d->A, r, d_point, d_list);
+        e = cudaMemcpyAsync(neighbors, d_list,
+                            sizeof(int) * static_cast<size_t>(std::min(total, cap)),
+                            cudaMemcpyDeviceToHost, d->stream);
+    }
     if (e == cudaSuccess)
         e = cudaStreamSynchronize(d->stream);
     dfree(d_point);
@@ -985,6 +1090,59 @@ int mdelast_driver_get_neighbors(mdelast_driver *d, int32_t *point, int32_t *nei
     if (e != cudaSuccess)
         return fail(MDELAST_ERR_CUDA, "neighbour readout: %s", cudaGetErrorString(e));
     return MDELAST_OK;
+}
+
+extern "C" {
+
+int mdelast_driver_get_observables(mdelast_driver *d, mdelast_observables *out) {
+    return get_observables_r(d, 0, out);
+}
+
+int mdelast_driver_get_atoms(mdelast_driver *d, int32_t field, double *out) {
+    return get_atoms_r(d, 0, field, out);
+}
+
+int mdelast_driver_get_chain(mdelast_driver *d, int32_t which, double *q, double *p_eta,
+                             double *eta, int32_t *nchain) {
+    return get_chain_r(d, 0, which, q, p_eta, eta, nchain);
+}
+
+int mdelast_driver_get_neighbors(mdelast_driver *d, int32_t *point, int32_t *neighbors,
+                                 int64_t cap, int64_t *n_entries) {
+    return get_neighbors_r(d, 0, point, neighbors, cap, n_entries);
+}
+
+int mdelast_batch_create(const mdelast_driver_config *cfgs, int32_t n_replicas,
+                         mdelast_driver **out) {
+    return create_system(cfgs, n_replicas, out);
+}
+
+int mdelast_batch_size(const mdelast_driver *d, int32_t *n_replicas, int64_t *n_atoms) {
+    if (!d)
+        return fail(MDELAST_ERR_ARGUMENT, "null driver");
+    if (n_replicas)
+        *n_replicas = d->n_rep;
+    if (n_atoms)
+        *n_atoms = d->N;
+    return MDELAST_OK;
+}
+
+int mdelast_batch_get_observables(mdelast_driver *d, int32_t replica, mdelast_observables *out) {
+    return get_observables_r(d, replica, out);
+}
+
+int mdelast_batch_get_atoms(mdelast_driver *d, int32_t replica, int32_t field, double *out) {
+    return get_atoms_r(d, replica, field, out);
+}
+
+int mdelast_batch_get_chain(mdelast_driver *d, int32_t replica, int32_t which, double *q,
+                            double *p_eta, double *eta, int32_t *nchain) {
+    return get_chain_r(d, replica, which, q, p_eta, eta, nchain);
+}
+
+int mdelast_batch_get_neighbors(mdelast_driver *d, int32_t replica, int32_t *point,
+                                int32_t *neighbors, int64_t cap, int64_t *n_entries) {
+    return get_neighbors_r(d, replica, point, neighbors, cap, n_entries);
 }
 
 int mdelast_driver_pair_correlation(mdelast_driver *d, int32_t mode) {

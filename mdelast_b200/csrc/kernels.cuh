@@ -26,6 +26,7 @@ void launch_force_mx(bool obs, bool kick, int tpa, int grid, cudaStream_t s, Ato
 __global__ void k_posf(AtomsView A);
 __global__ void k_kick_drift(AtomsView A, TablesView T);
 __global__ void k_pre(AtomsView A);
+__global__ void k_reduce(AtomsView A);
 __global__ void k_post(AtomsView A, int mode, int obs);
 __global__ void k_readout(AtomsView A, TablesView T, int r, int field, double *out,
                           const double *pos0, int stepped);

@@ -470,6 +470,168 @@ py::array_t<double> vec6(double const *v) {
     return a;
 }
 
+py::dict obs_dict(mdelast_observables const &o) {
+    py::dict d;
+    d["epot_eam_atom"] = o.epot_eam_atom;
+    d["epot_atom"] = o.epot_atom;
+    d["ekin_atom"] = o.ekin_atom;
+    d["etot_atom"] = o.etot_atom;
+    d["etot_cons"] = o.etot_cons;
+    d["etot_cons_err"] = o.etot_cons_err;
+    d["virial"] = o.virial;
+    d["total_laplacian"] = o.total_laplacian;
+    d["total_force2"] = o.total_force2;
+    d["temperature_kin"] = o.temperature_kin;
+    d["temperature_conf_inverse"] = o.temperature_conf_inverse;
+    d["pressure"] = o.pressure;
+    d["time"] = o.time;
+    d["cycle"] = static_cast<unsigned long long>(o.cycle);
+    d["born_stress_tensor"] = vec6(o.born_stress_tensor);
+    d["stress_tensor"] = vec6(o.stress_tensor);
+    py::array_t<double> cb({6, 6});
+    std::copy(o.born_elasticity_tensor, o.born_elasticity_tensor + 36, cb.mutable_data());
+    d["born_elasticity_tensor"] = cb;
+    d["volume"] = o.box[0] * (o.box[4] * o.box[8]);
+    d["box"] = py::make_tuple(o.box[0], o.box[4], o.box[8]);
+    d["baro_epsilon"] = o.baro_epsilon;
+    d["baro_p_epsilon"] = o.baro_p_epsilon;
+    d["status"] = o.status;
+    return d;
+}
+
+// Many independent replicas sharing one potential, advanced together on one GPU (new in
+// this implementation; the reference runs replicas as separate processes). Per replica:
+// positions (N,3) and velocities (N,3) arrays [cgs], types, ensemble, thermostat and
+// barostat, box edges, Nf; shared: potentials, masses, dt, list settings, precision.
+class BatchedMDDriver {
+  public:
+    BatchedMDDriver(std::vector<py::array_t<double, py::array::c_style | py::array::forcecast>> const &positions,
+                    std::vector<py::array_t<double, py::array::c_style | py::array::forcecast>> const &velocities,
+                    std::vector<std::vector<unsigned>> const &types,
+                    std::vector<PotentialPtr> const &pot, std::vector<EAMPtr> const &eam,
+                    std::vector<Ensamble> const &ensembles, std::vector<Thermostat> const &thermostats,
+                    std::vector<Barostat> const &barostats, std::vector<Box> const &boxes,
+                    std::vector<double> const &Nf, std::vector<double> const &mass, double dt,
+                    bool neighbors, double r_skin, double fatal_conservation,
+                    std::string const &precision, int device, std::vector<double> const &rg)
+        : pot_(pot), eam_(eam), mass_(mass) {
+        size_t const R = positions.size();
+        if (R == 0 || velocities.size() != R || types.size() != R || ensembles.size() != R ||
+            thermostats.size() != R || barostats.size() != R || boxes.size() != R ||
+            Nf.size() != R)
+            throw py::value_error("every per-replica list needs one entry per replica");
+        std::vector<mdelast_pair const *> ph;
+        for (auto const &p : pot)
+            ph.push_back(p->handle());
+        std::vector<mdelast_eam const *> eh;
+        for (auto const &e : eam)
+            eh.push_back(e->handle());
+        std::vector<mdelast_driver_config> cfg(R);
+        std::string const prec = precision.empty() ? default_precision : precision;
+        for (size_t r = 0; r < R; ++r) {
+            auto const &P = positions[r];
+            auto const &V = velocities[r];
+            size_t const N = types[r].size();
+            if (P.size() != static_cast<py::ssize_t>(3 * N) || V.size() != static_cast<py::ssize_t>(3 * N))
+                throw py::value_error("positions/velocities of a replica must be (N, 3)");
+            mdelast_driver_config &c = cfg[r];
+            c = mdelast_driver_config{};
+            c.n_atoms = static_cast<int32_t>(N);
+            c.n_types = static_cast<int32_t>(mass.size());
+            c.positions = P.data();
+            c.velocities = V.data();
+            c.types = reinterpret_cast<uint32_t const *>(types[r].data());
+            c.mass = mass_.data();
+            c.pair = ph.data();
+            c.eam = eh.data();
+            c.n_eam = static_cast<int32_t>(eh.size());
+            c.ensemble = ensembles[r];
+            c.coupling = MDELAST_THERMOSTAT_KINETIC;
+            Thermostat const &th = thermostats[r];
+            Barostat const &b = barostats[r];
+            c.thermo_T = th.temperature;
+            c.thermo_nchain = static_cast<int32_t>(th.nchain);
+            c.thermo_q = th.q.data();
+            c.thermo_p_eta = th.p_eta.data();
+            c.thermo_Nf = th.Nf;
+            c.baro_P = b.pressure;
+            c.baro_w = b.w;
+            c.baro_p_eps = b.p_epsilon;
+            c.baro_thermo_T = b.thermostat.temperature;
+            c.baro_nchain = static_cast<int32_t>(b.thermostat.nchain);
+            c.baro_q = b.thermostat.q.data();
+            c.baro_p_eta = b.thermostat.p_eta.data();
+            c.baro_Nf = b.thermostat.Nf;
+            for (int k = 0; k < 9; ++k)
+                c.box[k] = boxes[r].h[k];
+            c.n_rg = static_cast<int32_t>(rg.size());
+            c.rg = rg.data();
+            c.Nf = Nf[r];
+            c.dt = dt;
+            c.neighbors = neighbors ? 1 : 0;
+            c.r_skin = r_skin;
+            c.fatal_conservation = fatal_conservation;
+            c.precision = prec == "mixed" ? MDELAST_PRECISION_MIXED : MDELAST_PRECISION_FP64;
+            c.device = device;
+            counts_.push_back(N);
+        }
+        mdelast_driver *d = nullptr;
+        check_ni(mdelast_batch_create(cfg.data(), static_cast<int32_t>(R), &d));
+        d_ = d;
+    }
+    ~BatchedMDDriver() { mdelast_driver_destroy(d_); }
+    BatchedMDDriver(BatchedMDDriver const &) = delete;
+    BatchedMDDriver &operator=(BatchedMDDriver const &) = delete;
+
+    int n_replicas() const { return static_cast<int>(counts_.size()); }
+    long n_atoms() const {
+        long s = 0;
+        for (size_t n : counts_)
+            s += static_cast<long>(n);
+        return s;
+    }
+    double run(int n, int rebuild_every, int sample_every, bool timed) {
+        float ms = 0.f;
+        check(mdelast_driver_run(d_, n, rebuild_every, sample_every, timed ? &ms : nullptr));
+        return ms;
+    }
+    void integrate() { check(mdelast_driver_integrate(d_, 1)); }
+    void calculate_neighbors() { check_ni(mdelast_driver_calculate_neighbors(d_)); }
+    void set_sample(bool f) { check(mdelast_driver_set_sample_observables(d_, f ? 1 : 0)); }
+    bool get_sample() const {
+        int32_t f = 0;
+        check(mdelast_driver_get_sample_observables(d_, &f));
+        return f != 0;
+    }
+    py::dict observables(int r) {
+        mdelast_observables o;
+        check(mdelast_batch_get_observables(d_, r, &o));
+        return obs_dict(o);
+    }
+    py::array_t<double> atoms(int r, int field) {
+        if (r < 0 || r >= n_replicas())
+            throw py::index_error("replica index out of range");
+        size_t const N = counts_[static_cast<size_t>(r)];
+        bool const three = field <= MDELAST_ATOM_FORCES;
+        py::array_t<double> a = three ? py::array_t<double>({N, size_t(3)}) : py::array_t<double>(N);
+        check(mdelast_batch_get_atoms(d_, r, field, a.mutable_data()));
+        return a;
+    }
+    std::vector<double> kernel_times(int n) {
+        std::vector<double> t(MDELAST_N_KERNEL_TIMES);
+        check(mdelast_driver_kernel_times(d_, n, t.data()));
+        return t;
+    }
+    void synchronize() { check(mdelast_driver_synchronize(d_)); }
+
+  private:
+    mdelast_driver *d_ = nullptr;
+    std::vector<PotentialPtr> pot_;
+    std::vector<EAMPtr> eam_;
+    std::vector<double> mass_;
+    std::vector<size_t> counts_;
+};
+
 } // namespace
 
 PYBIND11_MAKE_OPAQUE(std::vector<PotentialPtr>);
@@ -615,6 +777,34 @@ PYBIND11_MODULE(md_driver_module, m) {
              "scalar, list build")
         .def_readonly("precision", &MDDriver::precision_)
         .def_property_readonly("status", [](MDDriver &d) { return d.obs().status; });
+
+    py::class_<BatchedMDDriver, std::shared_ptr<BatchedMDDriver>>(m, "BatchedMDDriver")
+        .def(py::init<std::vector<py::array_t<double, py::array::c_style | py::array::forcecast>> const &,
+                      std::vector<py::array_t<double, py::array::c_style | py::array::forcecast>> const &,
+                      std::vector<std::vector<unsigned>> const &, std::vector<PotentialPtr> const &,
+                      std::vector<EAMPtr> const &, std::vector<Ensamble> const &,
+                      std::vector<Thermostat> const &, std::vector<Barostat> const &,
+                      std::vector<Box> const &, std::vector<double> const &,
+                      std::vector<double> const &, double, bool, double, double,
+                      std::string const &, int, std::vector<double> const &>(),
+             py::arg("positions"), py::arg("velocities"), py::arg("types"), py::arg("pot"),
+             py::arg("eam"), py::arg("ensembles"), py::arg("thermostats"), py::arg("barostats"),
+             py::arg("boxes"), py::arg("Nf"), py::arg("mass"), py::arg("dt_global"),
+             py::arg("neighbors") = true, py::arg("r_skin") = 1.2,
+             py::arg("fatal_conservation") = 1e3, py::arg("precision") = "",
+             py::arg("device") = 0,
+             py::arg("rg") = std::vector<double>{1e-10, 2e-10})
+        .def_property_readonly("n_replicas", &BatchedMDDriver::n_replicas)
+        .def_property_readonly("n_atoms", &BatchedMDDriver::n_atoms)
+        .def("run", &BatchedMDDriver::run, py::arg("n_steps"), py::arg("rebuild_every") = 20,
+             py::arg("sample_every") = 1, py::arg("timed") = false)
+        .def("integrate", &BatchedMDDriver::integrate)
+        .def("calculate_neighbors", &BatchedMDDriver::calculate_neighbors)
+        .def_property("sample_observables", &BatchedMDDriver::get_sample, &BatchedMDDriver::set_sample)
+        .def("observables", &BatchedMDDriver::observables, py::arg("replica"))
+        .def("atoms", &BatchedMDDriver::atoms, py::arg("replica"), py::arg("field"))
+        .def("kernel_times", &BatchedMDDriver::kernel_times, py::arg("n_steps") = 10)
+        .def("synchronize", &BatchedMDDriver::synchronize);
 
     py::class_<Box, std::shared_ptr<Box>>(m, "Box")
         .def(py::init<py::array_t<double, py::array::c_style | py::array::forcecast>>())

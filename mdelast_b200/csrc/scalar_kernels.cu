@@ -23,11 +23,11 @@ constexpr double kBoltz = 1.38064852e-16; // units.hpp:7
 // expx_exact is the reference's formula: the library exp, then op = (1 - e)/x, or for
 // |x| <= 1e-3 the reference's own 5th-order Taylor polynomial of op.
 //
-// expx_series evaluates both functions from their Taylor series, exp(-x) = sum (-x)^k/k!
-// and op(x) = sum (-x)^k/(k+1)!, to degree 11, by Estrin's scheme. For |x| <= 1/16 the
-// first omitted term is below 1e-23 relative, so both agree with the exact values to the
-// last bit or two (and op avoids the cancellation of 1 - e). It has no branch, so the
-// independent exponentials of a chain sweep can be interleaved; thermostat arguments are
+// expx_series evaluates op from its Taylor series op(x) = sum (-x)^k/(k+1)! to degree 11
+// by Estrin's scheme (for |x| <= 1/16 the first omitted term is below 1e-23 relative, and
+// there is no cancellation of 1 - e), and exp(-x) = 1 - x op(x) with one FMA: both agree
+// with the exact values to the last bit or two. It has no branch, so the independent
+// exponentials of a chain sweep can be interleaved; thermostat arguments are
 // x = dt p_eta/Q ~ dt/tau, far inside the series range. expx_operator takes the series
 // and falls back to expx_exact outside |x| <= 1/16.
 __device__ __forceinline__ void expx_exact(double x, double &expx, double &op) {
@@ -41,18 +41,16 @@ __device__ __forceinline__ void expx_exact(double x, double &expx, double &op) {
 
 constexpr double kSeriesMax = 0.0625;
 
+// op from its series; exp(-x) = 1 - x op(x) then follows with one FMA and no
+// cancellation, since x op(x) = 1 - exp(-x) is small.
 __device__ __forceinline__ void expx_series(double x, double &expx, double &op) {
     double const y = -x, y2 = y * y, y4 = y2 * y2, y8 = y4 * y4;
-    double const a0 = 1.0 + y, a1 = fma(y, 1.0 / 6.0, 0.5),
-                 a2 = fma(y, 1.0 / 120.0, 1.0 / 24.0), a3 = fma(y, 1.0 / 5040.0, 1.0 / 720.0),
-                 a4 = fma(y, 1.0 / 362880.0, 1.0 / 40320.0),
-                 a5 = fma(y, 1.0 / 39916800.0, 1.0 / 3628800.0);
-    expx = fma(y8, fma(y2, a5, a4), fma(y4, fma(y2, a3, a2), fma(y2, a1, a0)));
     double const b0 = fma(y, 0.5, 1.0), b1 = fma(y, 1.0 / 24.0, 1.0 / 6.0),
                  b2 = fma(y, 1.0 / 720.0, 1.0 / 120.0), b3 = fma(y, 1.0 / 40320.0, 1.0 / 5040.0),
                  b4 = fma(y, 1.0 / 3628800.0, 1.0 / 362880.0),
                  b5 = fma(y, 1.0 / 479001600.0, 1.0 / 39916800.0);
     op = fma(y8, fma(y2, b5, b4), fma(y4, fma(y2, b3, b2), fma(y2, b1, b0)));
+    expx = fma(-x, op, 1.0);
 }
 
 __device__ __forceinline__ void expx_operator(double x, double &expx, double &op) {
@@ -322,36 +320,62 @@ __global__ void k_pre(AtomsView A) {
 // calculate_configurational_temperature), U2p and the NHC half steps (md_driver.cpp:
 // 583-595), and calculate_thermodynamics (md_driver.cpp:648-730). POST_INIT does the
 // part of the constructor after calculate_forces (md_driver.cpp:114-118).
+// Block sums of the density and force passes folded in chunks of kChunk blocks: block
+// (c, r) adds blocks [c kChunk, (c+1) kChunk) of replica r for every slot, in a fixed
+// order, spreading the reduction over many SMs (k_post then adds the chunk sums).
+__global__ void k_reduce(AtomsView A) {
+    Replica const *R = A.rep + blockIdx.y;
+    int const c = blockIdx.x;
+    int const g = threadIdx.x >> 6, q = threadIdx.x & 63;
+    __shared__ double part[4][64];
+    double a = 0.;
+    if (q < F_NSUM + D_NSUM) {
+        bool const fpass = q < F_NSUM;
+        int const ns = fpass ? F_NSUM : D_NSUM;
+        int const col = fpass ? q : q - F_NSUM;
+        double const *P = fpass ? A.pf : A.pd;
+        long const b0 = fpass ? R->fblk_begin : R->dblk_begin;
+        int const nb = fpass ? R->fblk_n : R->dblk_n;
+        int const lo = c * kChunk, hi = lo + kChunk < nb ? lo + kChunk : nb;
+#pragma unroll
+        for (int k = 0; k < kChunk / 4; ++k) {
+            int const b = lo + g + 4 * k;
+            if (b < hi)
+                a += P[(b0 + b) * ns + col];
+        }
+    }
+    part[g][q] = a;
+    __syncthreads();
+    if (threadIdx.x < 64)
+        A.red[(static_cast<size_t>(blockIdx.y) * A.max_chunks + c) * 64 + q] =
+            (part[0][q] + part[1][q]) + (part[2][q] + part[3][q]);
+}
+
 __global__ void k_post(AtomsView A, int mode, int obs) {
     Replica *R = A.rep + blockIdx.x;
     __shared__ double sf[F_NSUM], sd[D_NSUM];
     __shared__ double s_part[4][F_NSUM + D_NSUM];
     __shared__ double s_S, s_ekin, s_virial;
     int const t = threadIdx.x;
-    // Block sums of the two passes: 4 groups of 64 threads, thread (g, q) adds slot q over
-    // blocks g, g+4, ... with four independent accumulators; the group totals are then
-    // added in a fixed order, so the result does not depend on timing.
+    // Chunk sums of the two passes (k_reduce): 4 groups of 64 threads, thread (g, q) adds
+    // slot q over chunks g, g+4, ...; the group totals are then added in a fixed order, so
+    // the result does not depend on timing.
     {
         int const g = t >> 6, q = t & 63;
         int const nslot = F_NSUM + D_NSUM;
         if (q < nslot) {
-            bool const fpass = q < F_NSUM;
-            int const ns = fpass ? F_NSUM : D_NSUM;
-            int const col = fpass ? q : q - F_NSUM;
-            double const *P = fpass ? A.pf : A.pd;
-            long const b0 = fpass ? R->fblk_begin : R->dblk_begin;
-            int const nb = fpass ? R->fblk_n : R->dblk_n;
-            double a0 = 0., a1 = 0., a2 = 0., a3 = 0.;
-            int b = g;
-            for (; b + 12 < nb; b += 16) {
-                a0 += P[(b0 + b) * ns + col];
-                a1 += P[(b0 + b + 4) * ns + col];
-                a2 += P[(b0 + b + 8) * ns + col];
-                a3 += P[(b0 + b + 12) * ns + col];
+            int const nb = R->fblk_n > R->dblk_n ? R->fblk_n : R->dblk_n;
+            int const nc = (nb + kChunk - 1) / kChunk;
+            double const *P = A.red + static_cast<size_t>(blockIdx.x) * A.max_chunks * 64;
+            double a0 = 0., a1 = 0.;
+            int c = g;
+            for (; c + 4 < nc; c += 8) {
+                a0 += P[c * 64 + q];
+                a1 += P[(c + 4) * 64 + q];
             }
-            for (; b < nb; b += 4)
-                a0 += P[(b0 + b) * ns + col];
-            s_part[g][q] = (a0 + a1) + (a2 + a3);
+            for (; c < nc; c += 4)
+                a0 += P[c * 64 + q];
+            s_part[g][q] = a0 + a1;
         }
         __syncthreads();
         if (t < nslot) {
