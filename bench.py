@@ -186,16 +186,17 @@ def run_ours(args, rank, world, local_rank):
     e2e_steps = max(args.steps, REBUILD)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    bb = make_batch(m, t, cells, dt=DT, r_skin=SKIN, precision=args.precision,
-                    device=local_rank)
-    for s in range(e2e_steps):
-        bb.run(1, REBUILD, 1, False)
+    if not args.no_e2e:
+        bb = make_batch(m, t, cells, dt=DT, r_skin=SKIN, precision=args.precision,
+                        device=local_rank)
+        for s in range(e2e_steps):
+            bb.run(1, REBUILD, 1, False)
+            for r in range(bb.n_replicas):
+                _ = bb.observables(r)
         for r in range(bb.n_replicas):
-            _ = bb.observables(r)
-    for r in range(bb.n_replicas):
-        _ = (bb.atoms(r, m.ATOM_POSITIONS), bb.atoms(r, m.ATOM_VELOCITIES))
+            _ = (bb.atoms(r, m.ATOM_POSITIONS), bb.atoms(r, m.ATOM_VELOCITIES))
+        del bb
     t_e2e = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device="cuda")
-    del bb
     if dist is not None:
         dist.all_reduce(t_e2e, op=dist.ReduceOp.MAX)
     e2e_value = atoms_all * e2e_steps / float(t_e2e.item())
@@ -225,9 +226,10 @@ def run_ours(args, rank, world, local_rank):
         "plain_fp64_single_cell": plain,
         "roofline": roof,
         "cpu_baseline": cpu,
-        "e2e": {"value": e2e_value, "unit": "atom-steps/s",
-                "h2d_bytes_per_step": h2d / e2e_steps, "d2h_bytes_per_step": d2h / e2e_steps,
-                "steps": e2e_steps, "api": "md_driver_module.BatchedMDDriver"},
+        "e2e": None if args.no_e2e else {
+            "value": e2e_value, "unit": "atom-steps/s",
+            "h2d_bytes_per_step": h2d / e2e_steps, "d2h_bytes_per_step": d2h / e2e_steps,
+            "steps": e2e_steps, "api": "md_driver_module.BatchedMDDriver"},
         "gpu_launches": launches,
         "clocks": clocks,
     }
@@ -349,6 +351,7 @@ def main():
     ap.add_argument("--precision", choices=("fp64", "mixed"), default="mixed")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
