@@ -262,9 +262,12 @@ def half_list_nbar(m, t, cell):
     return float(point[-1]) / cell.n_atoms
 
 
-# ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_force launch of this workload
-# (profiles/k_force_cuzn6_13500.md); None until captured
-TRAFFIC_PER_LAUNCH: dict = {}
+# ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_force_mx launch
+# (profiles/k_force_mx_k_density_mx_bench_4x13500.md, 4 replicas, cold caches); the
+# 16- and 32-replica entries scale it by the atoms processed. None where not captured.
+_TRAFFIC_4 = 53.228288e6 + 0.228352e6
+TRAFFIC_PER_LAUNCH: dict = {("mixed", 4): _TRAFFIC_4, ("mixed", 16): 4 * _TRAFFIC_4,
+                            ("mixed", 32): 8 * _TRAFFIC_4}
 
 
 # ----------------------------------------------------------------------------- reference

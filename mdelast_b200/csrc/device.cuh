@@ -8,8 +8,9 @@
 //   vel   double[3][n_pad] velocities (SoA), times Replica::vscale (deferred NHC factor)
 //   frc   double[3][n_pad] forces
 //   rho, Fe, epot double[n_pad]; dF2 double2[n_pad] = (F'(rho), F''(rho))
-//   nbr   int[maxn][n_pad] full neighbour list, slot-major for coalesced index loads:
-//                          partners j > i from slot 0 up (n_up), j < i from maxn-1 down
+//   nbr   int[n_pad][maxn] full neighbour list, atom-major (one contiguous row per atom,
+//                          read by the atom's TPA lanes together): partners j > i from
+//                          slot 0 up (n_up), j < i from slot maxn-1 down (n_dn)
 //   rb    double[npot][nri][18] r-table bundle of each type pair (a <= b):
 //                          phi_ab | rho_a | rho_b quintic coefficients of one interval
 //   Ft    double[ntypes][nfi][6] embedding-function coefficients
