@@ -259,7 +259,14 @@ int mdelast_batch_get_neighbors(mdelast_driver *d, int32_t replica, int32_t *poi
  * 1 calculate_pair_correlations, 2 calculate_partial_pair_correlation. gr has n_rg
  * values, gr_partial n_types(n_types+1)/2 x n_rg. */
 int mdelast_driver_pair_correlation(mdelast_driver *d, int32_t mode);
+/* Copies the last results: gr (n_rg) and gr_partial (n_types(n_types+1)/2 rows of n_rg,
+ * row a + b(b+1)/2 for types a <= b); either may be NULL. Before any calculation, and for
+ * the part a mode did not compute, the previous values (initially zeros), as the
+ * reference's gr / gr_partial attributes. */
 int mdelast_driver_get_gr(mdelast_driver *d, double *gr, double *gr_partial);
+/* The same for replica `replica` of a batch, with that replica's rg. */
+int mdelast_batch_pair_correlation(mdelast_driver *d, int32_t replica, int32_t mode);
+int mdelast_batch_get_gr(mdelast_driver *d, int32_t replica, double *gr, double *gr_partial);
 
 #ifdef __cplusplus
 }

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "host_tables.h"
+#include "gr_kernels.cuh"
 #include "kernels.cuh"
 
 using namespace mdelast;
@@ -156,6 +157,15 @@ struct mdelast_driver_s {
     int *d_tmp_i = nullptr;
     size_t tmp_i_cap = 0;
 
+    // g(r) of each replica (md_driver.cpp:732-862): bin centres, results and counters on
+    // the device; replica r's rg and gr start at gr_off[r], its partial rows at npot * gr_off[r]
+    std::vector<long> gr_off;
+    std::vector<int> gr_n;
+    std::vector<double> gr_drg, gr_rmax;
+    double *d_rg = nullptr, *d_gr = nullptr, *d_grp = nullptr;
+    unsigned long long *d_gr_counts = nullptr;
+    int *d_gr_ntype = nullptr;
+
     AtomsView A{};
     TablesView T{};
     mdelast_observables *h_obs = nullptr; // pinned, n_rep entries
@@ -220,6 +230,11 @@ mdelast_driver_s::~mdelast_driver_s() {
     dfree(d_tmp_i);
     dfree(d_dblk_rep);
     dfree(d_fblk_rep);
+    dfree(d_rg);
+    dfree(d_gr);
+    dfree(d_grp);
+    dfree(d_gr_counts);
+    dfree(d_gr_ntype);
     if (stream)
         cudaStreamDestroy(stream);
 }
@@ -472,6 +487,8 @@ static int check_config(mdelast_driver_config const &c, mdelast_driver_config co
         return fail(MDELAST_ERR_ARGUMENT, "thermostat chains need 1..%d links", kMaxChain);
     if (c.n_rg < 2 || !c.rg)
         return fail(MDELAST_ERR_ARGUMENT, "rg needs at least 2 bins");
+    if (!(c.rg[0] > 0.) || !(c.rg[1] > c.rg[0])) // md_driver.cpp:86-87
+        return fail(MDELAST_ERR_ARGUMENT, "rg must be cell centred: rg[0] > 0, rg[1] > rg[0]");
     for (int a = 0; a < 3; ++a)
         for (int b = 0; b < 3; ++b)
             if (a != b && c.box[3 * a + b] != 0.)
@@ -684,6 +701,32 @@ static int create_system(const mdelast_driver_config *cfgs, int n_rep, mdelast_d
         }
         for (int t = 0; t < nt; ++t)
             T.feam_rcut[t] = static_cast<float>(T.eam_rcut[t] / kAng);
+    }
+
+    // ---- g(r) bins of each replica (md_driver.cpp:41): drg = rg[1] - rg[0],
+    // rmaxg = rg[n - 1] + drg / 2
+    {
+        long off = 0;
+        size_t max_slots = 0;
+        std::vector<double> rg_all;
+        for (int r = 0; r < n_rep; ++r) {
+            mdelast_driver_config const &c = cfgs[r];
+            d->gr_off.push_back(off);
+            d->gr_n.push_back(c.n_rg);
+            d->gr_drg.push_back(c.rg[1] - c.rg[0]);
+            d->gr_rmax.push_back(c.rg[c.n_rg - 1] + 0.5 * (c.rg[1] - c.rg[0]));
+            rg_all.insert(rg_all.end(), c.rg, c.rg + c.n_rg);
+            off += c.n_rg;
+            max_slots = std::max(max_slots, gr_count_slots(c.n_rg, nt));
+        }
+        TRY(dalloc(&d->d_rg, rg_all.size()));
+        TRY(dalloc(&d->d_gr, rg_all.size()));
+        TRY(dalloc(&d->d_grp, rg_all.size() * static_cast<size_t>(npot)));
+        TRY(dalloc(&d->d_gr_counts, max_slots));
+        TRY(dalloc(&d->d_gr_ntype, static_cast<size_t>(nt)));
+        if (cudaMemcpy(d->d_rg, rg_all.data(), sizeof(double) * rg_all.size(),
+                       cudaMemcpyHostToDevice))
+            return bail(fail(MDELAST_ERR_CUDA, "rg upload failed"));
     }
 
     // ---- replica states
@@ -1092,6 +1135,49 @@ static int get_neighbors_r(mdelast_driver *d, int r, int32_t *point, int32_t *ne
     return MDELAST_OK;
 }
 
+// md_driver.cpp:732-862 on the device: counts and normalises on the driver's stream after
+// the last step launched; get_gr_r waits for it.
+static int pair_correlation_r(mdelast_driver *d, int r, int32_t mode) {
+    clear_error();
+    if (!d || r < 0 || r >= d->n_rep || mode < 0 || mode > 2)
+        return fail(MDELAST_ERR_ARGUMENT, "bad argument");
+    CK(cudaSetDevice(d->device));
+    if (int rc = d->wait_step())
+        return rc;
+    GrArgs g{};
+    g.crd = d->d_crd + d->rep_begin[r];
+    g.rep = d->d_rep + r;
+    g.n = d->rep_count[r];
+    g.ntypes = d->ntypes;
+    g.n_rg = d->gr_n[r];
+    g.mode = mode;
+    g.rg = d->d_rg + d->gr_off[r];
+    g.drg = d->gr_drg[r];
+    g.rmaxg = d->gr_rmax[r];
+    g.counts = d->d_gr_counts;
+    g.n_per_type = d->d_gr_ntype;
+    g.gr = d->d_gr + d->gr_off[r];
+    g.gr_partial = d->d_grp + static_cast<size_t>(d->npot) * d->gr_off[r];
+    CK(gr_enqueue(g, d->stream));
+    return MDELAST_OK;
+}
+
+static int get_gr_r(mdelast_driver *d, int r, double *gr, double *gr_partial) {
+    clear_error();
+    if (!d || r < 0 || r >= d->n_rep)
+        return fail(MDELAST_ERR_ARGUMENT, "bad argument");
+    CK(cudaSetDevice(d->device));
+    size_t const n = static_cast<size_t>(d->gr_n[r]);
+    if (gr)
+        CK(cudaMemcpyAsync(gr, d->d_gr + d->gr_off[r], sizeof(double) * n,
+                           cudaMemcpyDeviceToHost, d->stream));
+    if (gr_partial)
+        CK(cudaMemcpyAsync(gr_partial, d->d_grp + static_cast<size_t>(d->npot) * d->gr_off[r],
+                           sizeof(double) * n * d->npot, cudaMemcpyDeviceToHost, d->stream));
+    CK(cudaStreamSynchronize(d->stream));
+    return MDELAST_OK;
+}
+
 extern "C" {
 
 int mdelast_driver_get_observables(mdelast_driver *d, mdelast_observables *out) {
@@ -1146,16 +1232,19 @@ int mdelast_batch_get_neighbors(mdelast_driver *d, int32_t replica, int32_t *poi
 }
 
 int mdelast_driver_pair_correlation(mdelast_driver *d, int32_t mode) {
-    (void)d;
-    (void)mode;
-    return fail(MDELAST_ERR_UNSUPPORTED, "pair correlation is not available yet");
+    return pair_correlation_r(d, 0, mode);
 }
 
 int mdelast_driver_get_gr(mdelast_driver *d, double *gr, double *gr_partial) {
-    (void)d;
-    (void)gr;
-    (void)gr_partial;
-    return fail(MDELAST_ERR_UNSUPPORTED, "pair correlation is not available yet");
+    return get_gr_r(d, 0, gr, gr_partial);
+}
+
+int mdelast_batch_pair_correlation(mdelast_driver *d, int32_t replica, int32_t mode) {
+    return pair_correlation_r(d, replica, mode);
+}
+
+int mdelast_batch_get_gr(mdelast_driver *d, int32_t replica, double *gr, double *gr_partial) {
+    return get_gr_r(d, replica, gr, gr_partial);
 }
 
 int mdelast_table_eval_device(const mdelast_pair *p, const mdelast_eam *e, int which,

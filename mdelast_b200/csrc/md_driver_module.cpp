@@ -293,6 +293,8 @@ class MDDriver {
         size_t const nt = mass.size();
         if (ph.size() != nt * (nt + 1) / 2)
             throw py::value_error("PotentialVector needs n_types (n_types + 1) / 2 entries");
+        gr.assign(rg.size(), 0.); // md_driver.cpp:39-40
+        gr_partial.assign(nt * (nt + 1) / 2, std::vector<double>(rg.size(), 0.));
         Nparticles_per_type.assign(nt, 0);
         for (unsigned t : types)
             if (t < nt)
@@ -578,6 +580,7 @@ class BatchedMDDriver {
         mdelast_driver *d = nullptr;
         check_ni(mdelast_batch_create(cfg.data(), static_cast<int32_t>(R), &d));
         d_ = d;
+        n_rg_ = rg.size();
     }
     ~BatchedMDDriver() { mdelast_driver_destroy(d_); }
     BatchedMDDriver(BatchedMDDriver const &) = delete;
@@ -623,9 +626,21 @@ class BatchedMDDriver {
         return t;
     }
     void synchronize() { check(mdelast_driver_synchronize(d_)); }
+    // g(r) of one replica (mode as MDDriver's three calculate_* methods: 0, 1, 2);
+    // returns (gr, gr_partial) with gr_partial one row per type pair a <= b
+    py::tuple pair_correlation(int r, int mode) {
+        if (r < 0 || r >= n_replicas())
+            throw py::index_error("replica index out of range");
+        check(mdelast_batch_pair_correlation(d_, r, mode));
+        size_t const nt = mass_.size(), np = nt * (nt + 1) / 2;
+        py::array_t<double> g(n_rg_), gp({np, n_rg_});
+        check(mdelast_batch_get_gr(d_, r, g.mutable_data(), gp.mutable_data()));
+        return py::make_tuple(g, gp);
+    }
 
   private:
     mdelast_driver *d_ = nullptr;
+    size_t n_rg_ = 0;
     std::vector<PotentialPtr> pot_;
     std::vector<EAMPtr> eam_;
     std::vector<double> mass_;
@@ -804,6 +819,8 @@ PYBIND11_MODULE(md_driver_module, m) {
         .def("observables", &BatchedMDDriver::observables, py::arg("replica"))
         .def("atoms", &BatchedMDDriver::atoms, py::arg("replica"), py::arg("field"))
         .def("kernel_times", &BatchedMDDriver::kernel_times, py::arg("n_steps") = 10)
+        .def("pair_correlation", &BatchedMDDriver::pair_correlation, py::arg("replica"),
+             py::arg("mode") = 1)
         .def("synchronize", &BatchedMDDriver::synchronize);
 
     py::class_<Box, std::shared_ptr<Box>>(m, "Box")

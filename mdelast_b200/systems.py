@@ -132,8 +132,12 @@ def make_driver(m, tables: SetflTables, cell: Cell, dt=2e-15, neighbors=True, r_
 
 
 def make_batch(m, tables: SetflTables, cells: list[Cell], dt=2e-15, neighbors=True,
-               r_skin=1.2, precision="fp64", device=0, fatal_conservation=1e3):
+               r_skin=1.2, precision="fp64", device=0, fatal_conservation=1e3, rg=None):
+    """One BatchedMDDriver over `cells`; g(r) bins `rg` shared by all replicas (default:
+    those of the smallest cell)."""
     _, pots, eams = make_objects(m, tables)
+    if rg is None:
+        rg = rg_bins(min(cells, key=lambda c: min(c.box)))
     ths, baros = zip(*[_thermostats(m, c) for c in cells])
     return m.BatchedMDDriver([c.positions for c in cells], [c.velocities for c in cells],
                              [[int(t) for t in c.types] for c in cells], m.PotentialVector(pots),
@@ -142,4 +146,4 @@ def make_batch(m, tables: SetflTables, cells: list[Cell], dt=2e-15, neighbors=Tr
                              [c.Nf for c in cells], list(tables.masses), dt,
                              neighbors=neighbors, r_skin=r_skin,
                              fatal_conservation=fatal_conservation, precision=precision,
-                             device=device)
+                             device=device, rg=list(rg))
