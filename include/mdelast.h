@@ -268,6 +268,39 @@ int mdelast_driver_get_gr(mdelast_driver *d, double *gr, double *gr_partial);
 int mdelast_batch_pair_correlation(mdelast_driver *d, int32_t replica, int32_t mode);
 int mdelast_batch_get_gr(mdelast_driver *d, int32_t replica, double *gr, double *gr_partial);
 
+/* g(r) that allocates nothing. No counterpart in the reference: it exists for callers
+ * that may not allocate device memory when they sample g(r), for example an application
+ * whose allocator owns all device memory and forbids third-party cudaMalloc/cudaFree, or
+ * a sampling loop that cannot take the device-wide synchronisation of a cudaFree.
+ *
+ * Same counting and normalisation as mdelast_driver_pair_correlation (md_driver.cpp:
+ * 732-862) and bit-identical results on the same coordinates, but on arrays the caller
+ * holds on the current device: coordinates (n_atoms x 3 scaled coordinates, as the
+ * MDELAST_ATOM_COORDINATES readout), types (n_atoms values in [0, n_types); atoms of other
+ * types are not counted), rg (n_rg evenly spaced bin centres, rg[0] > 0), and the outputs
+ * gr (n_rg, written for modes 0 and 1) and gr_partial (n_types(n_types+1)/2 rows of n_rg,
+ * written for modes 1 and 2; the other may be NULL). box: 3 edges of the diagonal box, in
+ * host memory. The work is queued on `stream` (a cudaStream_t; NULL is the default stream)
+ * and the call returns without waiting for it.
+ *
+ * Scratch: a fixed array in the library's device image holding
+ * (1 + n_types(n_types+1)/2) x n_rg 64-bit counters, at most MDELAST_GR_STATIC_MAX_SLOTS
+ * (512 KB), and n_types <= 8; larger requests return MDELAST_ERR_CAPACITY with the sizes
+ * in mdelast_last_error(). Nothing needs to start at zero: each call clears the counters it
+ * uses on `stream` before counting.
+ *
+ * The first call on a device does set-up (it loads the library's kernels on that device
+ * and looks up the scratch address with cudaGetSymbolAddress, with that device current);
+ * make it before any stream capture begins. There is ONE scratch array per device: calls
+ * that overlap on the same device (different streams, or different host threads, without
+ * ordering between them) race on it and give wrong counts; order them on one stream or
+ * with events. */
+#define MDELAST_GR_STATIC_MAX_SLOTS 65536
+int mdelast_pair_correlation_static(const double *coordinates, const uint32_t *types,
+                                    int32_t n_atoms, int32_t n_types, const double *box,
+                                    const double *rg, int32_t n_rg, int32_t mode, double *gr,
+                                    double *gr_partial, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
