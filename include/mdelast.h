@@ -268,6 +268,62 @@ int mdelast_driver_get_gr(mdelast_driver *d, double *gr, double *gr_partial);
 int mdelast_batch_pair_correlation(mdelast_driver *d, int32_t replica, int32_t mode);
 int mdelast_batch_get_gr(mdelast_driver *d, int32_t replica, double *gr, double *gr_partial);
 
+/* ---- Samples and fluctuation sums (molecular_dynamics.py:1218-1238, 663-1000) ----
+ *
+ * Every step that samples observables (sample_observables set, or the sampled steps of
+ * mdelast_driver_run) appends one record of what the reference's append_sample reads
+ * after that step (molecular_dynamics.py:1218-1238) to a ring on the device, one ring per
+ * replica. The host drains it when it wants the series, so a run needs no per-step
+ * readout. */
+typedef struct mdelast_sample {
+    double time, cycle;
+    double temperature_kin, temperature_conf_inverse, total_laplacian, total_force2;
+    double pressure;
+    double stress_tensor[6];
+    double etot_atom, epot_atom, epot_eam_atom, ekin_atom, etot_cons, etot_cons_err;
+    double born_stress_tensor[6];
+    double born_elasticity_tensor[21]; /* upper triangle, row by row (C11 C12 .. C16 C22 ..) */
+    double volume;                     /* box volume after the step */
+    double status;                     /* the status word after the step */
+} mdelast_sample;
+
+#define MDELAST_DEFAULT_SAMPLE_RING 1024
+/* (Re)allocate every replica's ring with room for `capacity` records (0: no ring);
+ * records not yet drained are dropped. A driver starts with MDELAST_DEFAULT_SAMPLE_RING. */
+int mdelast_driver_set_sample_ring(mdelast_driver *d, int32_t capacity);
+/* Copy the records written since the last drain, oldest first, at most `cap`; *n_out gets
+ * the number copied and *n_lost the number overwritten before they were drained. Records
+ * beyond `cap` stay for the next drain. */
+int mdelast_driver_drain_samples(mdelast_driver *d, mdelast_sample *out, int64_t cap,
+                                 int64_t *n_out, int64_t *n_lost);
+int mdelast_batch_drain_samples(mdelast_driver *d, int32_t replica, mdelast_sample *out,
+                                int64_t cap, int64_t *n_out, int64_t *n_lost);
+
+/* Running sums of the production window for the fluctuation formula of the elastic
+ * constants (molecular_dynamics.py:826-958), bulk modulus and thermal expansion
+ * (:776-824), updated on the device at every sampled step once started (Welford's
+ * updates in FP64). x = (born_stress_tensor[6], N/V, V, etot_atom). */
+typedef struct mdelast_fluct {
+    double n;                 /* samples accumulated */
+    double n_atoms;
+    double mean[9];           /* means of x */
+    double comoment[45];      /* sum (x_a - mean_a)(x_b - mean_b), a <= b, row by row */
+    double born_el_mean[21];  /* mean of born_elasticity_tensor (upper triangle) */
+} mdelast_fluct;
+/* Clear the sums of every replica and start accumulating from the next sampled step
+ * (the reference's samples_thermalization cut). */
+int mdelast_driver_fluct_start(mdelast_driver *d);
+int mdelast_driver_get_fluct(mdelast_driver *d, mdelast_fluct *out);
+int mdelast_batch_get_fluct(mdelast_driver *d, int32_t replica, mdelast_fluct *out);
+/* The reference's estimator (molecular_dynamics.py:776-824, 826-958) from the sums, on the
+ * host: C (6 x 6) = <C^B> - <V>/kT cov(s', s') + ideal-gas term (+ bulk modulus in the
+ * upper-left block for NPT), s' = sigma^B - (N kT / V) delta in NPT; kT = k_B T_thermostat.
+ * summary (6 values, may be NULL): C11, C12, C44 (component averages), bulk modulus,
+ * isothermal compressibility, volumetric thermal expansion (the last three 0 unless NPT).
+ * Needs at least 2 samples. */
+int mdelast_elastic_constants(const mdelast_fluct *f, int32_t ensemble, double T_thermostat,
+                              double P_barostat, double *C, double *summary);
+
 /* g(r) that allocates nothing. No counterpart in the reference: it exists for callers
  * that may not allocate device memory when they sample g(r), for example an application
  * whose allocator owns all device memory and forbids third-party cudaMalloc/cudaFree, or

@@ -75,6 +75,10 @@ struct Replica {
     Chain th, bth;
     mdelast_observables obs;
     int initialised, pad2;
+    // samples: records appended to the ring so far; fluctuation sums while acc_on
+    double n_samples;
+    int acc_on, pad3;
+    mdelast_fluct acc;
 };
 
 struct TablesView {
@@ -125,6 +129,8 @@ struct AtomsView {
     int cell_cap, n_cells;
     double r_list_sq;
     int *max_count; // [2]: largest neighbour count, largest cell count of the last build
+    mdelast_sample *ring; // [n_rep][ring_cap] records of sampled steps (or null)
+    int ring_cap, pad_ring;
 };
 
 // md_driver.hpp:48-50: round half away from zero through a truncating int conversion

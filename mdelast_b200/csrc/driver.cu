@@ -157,6 +157,10 @@ struct mdelast_driver_s {
     int *d_tmp_i = nullptr;
     size_t tmp_i_cap = 0;
 
+    // sample rings: [n_rep][ring_cap] records; records of replica r already drained
+    mdelast_sample *d_ring = nullptr;
+    std::vector<long long> drained;
+    int alloc_ring(int cap);
     // g(r) of each replica (md_driver.cpp:732-862): bin centres, results and counters on
     // the device; replica r's rg and gr start at gr_off[r], its partial rows at npot * gr_off[r]
     std::vector<long> gr_off;
@@ -230,6 +234,7 @@ mdelast_driver_s::~mdelast_driver_s() {
     dfree(d_tmp_i);
     dfree(d_dblk_rep);
     dfree(d_fblk_rep);
+    dfree(d_ring);
     dfree(d_rg);
     dfree(d_gr);
     dfree(d_grp);
@@ -261,6 +266,25 @@ int mdelast_driver_s::alloc_cells(int n_cells, int cell_cap) {
     cells_alloc = n_cells;
     A.cell_cap = cell_cap;
     drop_graphs();
+    return MDELAST_OK;
+}
+
+int mdelast_driver_s::alloc_ring(int cap) {
+    drop_graphs(); // the step graphs hold the ring pointer
+    dfree(d_ring);
+    A.ring = nullptr;
+    A.ring_cap = 0;
+    if (cap > 0) {
+        if (int rc = dalloc(&d_ring, static_cast<size_t>(n_rep) * cap))
+            return rc;
+        A.ring = d_ring;
+        A.ring_cap = cap;
+    }
+    drained.assign(static_cast<size_t>(n_rep), 0);
+    k_samples_reset<<<(n_rep + 63) / 64, 64, 0, stream>>>(A, 1);
+    CK(cudaGetLastError());
+    // complete before any host-side read-modify-write of the replica states
+    CK(cudaStreamSynchronize(stream));
     return MDELAST_OK;
 }
 
@@ -754,6 +778,7 @@ static int create_system(const mdelast_driver_config *cfgs, int n_rep, mdelast_d
         x.eps = 0.;
         x.p_eps = c.baro_p_eps;
         x.vscale = 1.;
+        x.acc.n_atoms = c.n_atoms;
         set_chain(x.th, c.thermo_T, c.thermo_nchain, c.thermo_q, c.thermo_p_eta, c.thermo_Nf);
         set_chain(x.bth, c.baro_thermo_T, c.baro_nchain, c.baro_q, c.baro_p_eta, c.baro_Nf);
         reps.push_back(&x);
@@ -832,6 +857,7 @@ static int create_system(const mdelast_driver_config *cfgs, int n_rep, mdelast_d
     A.dblk_rep = d->d_dblk_rep;
     A.fblk_rep = d->d_fblk_rep;
     A.max_count = d->d_max_count;
+    TRY(d->alloc_ring(MDELAST_DEFAULT_SAMPLE_RING));
     if (d->neighbors) // md_driver.cpp:42: pow<2>(pot[0]->rcut * r_skin)
         A.r_list_sq = (rcut * c0.r_skin) * (rcut * c0.r_skin);
     else
@@ -1178,7 +1204,97 @@ static int get_gr_r(mdelast_driver *d, int r, double *gr, double *gr_partial) {
     return MDELAST_OK;
 }
 
+// Records of replica r written since its last drain (molecular_dynamics.py:1218-1238).
+static int drain_samples_r(mdelast_driver *d, int r, mdelast_sample *out, int64_t cap,
+                           int64_t *n_out, int64_t *n_lost) {
+    clear_error();
+    if (!d || r < 0 || r >= d->n_rep || cap < 0 || (cap > 0 && !out))
+        return fail(MDELAST_ERR_ARGUMENT, "bad argument");
+    CK(cudaSetDevice(d->device));
+    if (int rc = d->wait_step())
+        return rc;
+    double written_d = 0.;
+    CK(cudaMemcpy(&written_d,
+                  reinterpret_cast<char *>(d->d_rep + r) + offsetof(Replica, n_samples),
+                  sizeof(double), cudaMemcpyDeviceToHost));
+    long long const written = static_cast<long long>(written_d);
+    long long const ringc = d->A.ring_cap;
+    long long &done = d->drained[static_cast<size_t>(r)];
+    long long const first = ringc > 0 ? std::max(done, written - ringc) : written;
+    long long const lost = first - done;
+    long long const count = std::min<long long>(written - first, cap);
+    mdelast_sample const *base = d->d_ring + static_cast<size_t>(r) * (ringc > 0 ? ringc : 0);
+    long long k = 0;
+    while (k < count) { // at most two contiguous pieces of the ring
+        long long const slot = (first + k) % ringc;
+        long long const len = std::min(count - k, ringc - slot);
+        CK(cudaMemcpyAsync(out + k, base + slot, sizeof(mdelast_sample) * len,
+                           cudaMemcpyDeviceToHost, d->stream));
+        k += len;
+    }
+    CK(cudaStreamSynchronize(d->stream));
+    done = first + count;
+    if (n_out)
+        *n_out = count;
+    if (n_lost)
+        *n_lost = lost;
+    return MDELAST_OK;
+}
+
+static int get_fluct_r(mdelast_driver *d, int r, mdelast_fluct *out) {
+    clear_error();
+    if (!d || !out || r < 0 || r >= d->n_rep)
+        return fail(MDELAST_ERR_ARGUMENT, "bad argument");
+    CK(cudaSetDevice(d->device));
+    if (int rc = d->wait_step())
+        return rc;
+    CK(cudaMemcpy(out, reinterpret_cast<char *>(d->d_rep + r) + offsetof(Replica, acc),
+                  sizeof(mdelast_fluct), cudaMemcpyDeviceToHost));
+    return MDELAST_OK;
+}
+
 extern "C" {
+
+int mdelast_driver_set_sample_ring(mdelast_driver *d, int32_t capacity) {
+    clear_error();
+    if (!d || capacity < 0)
+        return fail(MDELAST_ERR_ARGUMENT, "bad argument");
+    CK(cudaSetDevice(d->device));
+    if (int rc = d->wait_step())
+        return rc;
+    return d->alloc_ring(capacity);
+}
+
+int mdelast_driver_drain_samples(mdelast_driver *d, mdelast_sample *out, int64_t cap,
+                                 int64_t *n_out, int64_t *n_lost) {
+    return drain_samples_r(d, 0, out, cap, n_out, n_lost);
+}
+
+int mdelast_batch_drain_samples(mdelast_driver *d, int32_t replica, mdelast_sample *out,
+                                int64_t cap, int64_t *n_out, int64_t *n_lost) {
+    return drain_samples_r(d, replica, out, cap, n_out, n_lost);
+}
+
+int mdelast_driver_fluct_start(mdelast_driver *d) {
+    clear_error();
+    if (!d)
+        return fail(MDELAST_ERR_ARGUMENT, "null driver");
+    CK(cudaSetDevice(d->device));
+    if (int rc = d->wait_step())
+        return rc;
+    k_samples_reset<<<(d->n_rep + 63) / 64, 64, 0, d->stream>>>(d->A, 2);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(d->stream));
+    return MDELAST_OK;
+}
+
+int mdelast_driver_get_fluct(mdelast_driver *d, mdelast_fluct *out) {
+    return get_fluct_r(d, 0, out);
+}
+
+int mdelast_batch_get_fluct(mdelast_driver *d, int32_t replica, mdelast_fluct *out) {
+    return get_fluct_r(d, replica, out);
+}
 
 int mdelast_driver_get_observables(mdelast_driver *d, mdelast_observables *out) {
     return get_observables_r(d, 0, out);

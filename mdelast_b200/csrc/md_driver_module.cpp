@@ -45,6 +45,101 @@ void check_ni(int rc) {
     check(rc);
 }
 
+// Every record of the sample ring of replica r (r < 0: a single driver), as arrays named
+// like the attributes molecular_dynamics.py:1218-1238 appends per sampled step.
+py::dict drain_dict(mdelast_driver *d, int r) {
+    std::vector<mdelast_sample> all, buf(4096);
+    int64_t lost_total = 0;
+    for (;;) {
+        int64_t n = 0, lost = 0;
+        int64_t const cap = static_cast<int64_t>(buf.size());
+        check(r < 0 ? mdelast_driver_drain_samples(d, buf.data(), cap, &n, &lost)
+                    : mdelast_batch_drain_samples(d, r, buf.data(), cap, &n, &lost));
+        lost_total += lost;
+        all.insert(all.end(), buf.begin(), buf.begin() + n);
+        if (n < cap)
+            break;
+    }
+    size_t const n = all.size();
+    py::dict out;
+    auto col = [&](char const *name, double mdelast_sample::*f) {
+        py::array_t<double> a(n);
+        for (size_t i = 0; i < n; ++i)
+            a.mutable_data()[i] = all[i].*f;
+        out[name] = a;
+    };
+    col("time", &mdelast_sample::time);
+    col("cycle", &mdelast_sample::cycle);
+    col("temperature_kin", &mdelast_sample::temperature_kin);
+    col("temperature_conf_inverse", &mdelast_sample::temperature_conf_inverse);
+    col("total_laplacian", &mdelast_sample::total_laplacian);
+    col("total_force2", &mdelast_sample::total_force2);
+    col("pressure", &mdelast_sample::pressure);
+    col("etot_atom", &mdelast_sample::etot_atom);
+    col("epot_atom", &mdelast_sample::epot_atom);
+    col("epot_eam_atom", &mdelast_sample::epot_eam_atom);
+    col("ekin_atom", &mdelast_sample::ekin_atom);
+    col("etot_cons", &mdelast_sample::etot_cons);
+    col("etot_cons_err", &mdelast_sample::etot_cons_err);
+    col("volume", &mdelast_sample::volume);
+    py::array_t<double> st({n, size_t(6)}), bs({n, size_t(6)}), be({n, size_t(6), size_t(6)});
+    py::array_t<uint32_t> status(n);
+    for (size_t i = 0; i < n; ++i) {
+        for (int k = 0; k < 6; ++k) {
+            st.mutable_data()[6 * i + k] = all[i].stress_tensor[k];
+            bs.mutable_data()[6 * i + k] = all[i].born_stress_tensor[k];
+        }
+        int q = 0;
+        for (int a = 0; a < 6; ++a)
+            for (int b = 0; b < 6; ++b)
+                be.mutable_data()[36 * i + 6 * a + b] =
+                    b >= a ? all[i].born_elasticity_tensor[q++] : 0.;
+        status.mutable_data()[i] = static_cast<uint32_t>(all[i].status);
+    }
+    out["stress_tensor"] = st;
+    out["born_stress_tensor"] = bs;
+    out["born_elasticity_tensor"] = be;
+    out["status"] = status;
+    out["lost"] = lost_total;
+    return out;
+}
+
+py::dict fluct_dict(mdelast_fluct const &f) {
+    py::dict out;
+    out["n"] = f.n;
+    out["n_atoms"] = f.n_atoms;
+    py::array_t<double> mean(9), M({size_t(9), size_t(9)}), cb({size_t(6), size_t(6)});
+    std::copy(f.mean, f.mean + 9, mean.mutable_data());
+    int q = 0;
+    for (int a = 0; a < 9; ++a)
+        for (int b = a; b < 9; ++b, ++q)
+            M.mutable_data()[9 * a + b] = M.mutable_data()[9 * b + a] = f.comoment[q];
+    q = 0;
+    for (int a = 0; a < 6; ++a)
+        for (int b = 0; b < 6; ++b)
+            cb.mutable_data()[6 * a + b] = b >= a ? f.born_el_mean[q++] : 0.;
+    out["mean"] = mean;
+    out["comoment"] = M;
+    out["born_el_mean"] = cb;
+    return out;
+}
+
+py::dict elastic_dict(mdelast_fluct const &f, int ensemble, double T, double P) {
+    py::array_t<double> C({size_t(6), size_t(6)});
+    double sm[6];
+    check(mdelast_elastic_constants(&f, ensemble, T, P, C.mutable_data(), sm));
+    py::dict out;
+    out["C"] = C;
+    out["C11"] = sm[0];
+    out["C12"] = sm[1];
+    out["C44"] = sm[2];
+    out["bulk_modulus"] = sm[3];
+    out["compressibility"] = sm[4];
+    out["volume_thermal_expansion"] = sm[5];
+    out["n_samples"] = f.n;
+    return out;
+}
+
 int parse_interp(std::string const &name) {
     if (name == "quintic")
         return MDELAST_QUINTIC;
@@ -435,6 +530,20 @@ class MDDriver {
         }
     }
     void synchronize() { check(mdelast_driver_synchronize(d_)); }
+    void set_sample_ring(int capacity) { check(mdelast_driver_set_sample_ring(d_, capacity)); }
+    py::dict drain_samples() { return drain_dict(d_, -1); }
+    void fluctuation_start() { check(mdelast_driver_fluct_start(d_)); }
+    mdelast_fluct fluct() {
+        mdelast_fluct f;
+        check(mdelast_driver_get_fluct(d_, &f));
+        return f;
+    }
+    py::dict fluctuations() { return fluct_dict(fluct()); }
+    py::dict elastic_constants(py::object T, py::object P) {
+        return elastic_dict(fluct(), static_cast<int>(ensamble),
+                            T.is_none() ? thermo_T_ : T.cast<double>(),
+                            P.is_none() ? baro_P_ : P.cast<double>());
+    }
     double run(int n, int rebuild_every, int sample_every, bool timed) {
         float ms = 0.f;
         check(mdelast_driver_run(d_, n, rebuild_every, sample_every, timed ? &ms : nullptr));
@@ -576,6 +685,9 @@ class BatchedMDDriver {
             c.precision = prec == "mixed" ? MDELAST_PRECISION_MIXED : MDELAST_PRECISION_FP64;
             c.device = device;
             counts_.push_back(N);
+            ens_.push_back(c.ensemble);
+            T_.push_back(th.temperature);
+            P_.push_back(b.pressure);
         }
         mdelast_driver *d = nullptr;
         check_ni(mdelast_batch_create(cfg.data(), static_cast<int32_t>(R), &d));
@@ -628,6 +740,26 @@ class BatchedMDDriver {
     void synchronize() { check(mdelast_driver_synchronize(d_)); }
     // g(r) of one replica (mode as MDDriver's three calculate_* methods: 0, 1, 2);
     // returns (gr, gr_partial) with gr_partial one row per type pair a <= b
+    void set_sample_ring(int capacity) { check(mdelast_driver_set_sample_ring(d_, capacity)); }
+    py::dict drain_samples(int r) {
+        if (r < 0 || r >= n_replicas())
+            throw py::index_error("replica index out of range");
+        return drain_dict(d_, r);
+    }
+    void fluctuation_start() { check(mdelast_driver_fluct_start(d_)); }
+    mdelast_fluct fluct(int r) {
+        mdelast_fluct f;
+        check(mdelast_batch_get_fluct(d_, r, &f));
+        return f;
+    }
+    py::dict fluctuations(int r) { return fluct_dict(fluct(r)); }
+    py::dict elastic_constants(int r, py::object T, py::object P) {
+        if (r < 0 || r >= n_replicas())
+            throw py::index_error("replica index out of range");
+        size_t const k = static_cast<size_t>(r);
+        return elastic_dict(fluct(r), ens_[k], T.is_none() ? T_[k] : T.cast<double>(),
+                            P.is_none() ? P_[k] : P.cast<double>());
+    }
     py::tuple pair_correlation(int r, int mode) {
         if (r < 0 || r >= n_replicas())
             throw py::index_error("replica index out of range");
@@ -641,6 +773,8 @@ class BatchedMDDriver {
   private:
     mdelast_driver *d_ = nullptr;
     size_t n_rg_ = 0;
+    std::vector<int> ens_;
+    std::vector<double> T_, P_; // thermostat temperature and barostat pressure per replica
     std::vector<PotentialPtr> pot_;
     std::vector<EAMPtr> eam_;
     std::vector<double> mass_;
@@ -777,6 +911,17 @@ PYBIND11_MODULE(md_driver_module, m) {
         .def("calculate_pair_correlation", [](MDDriver &d) { d.pair_correlation(0); })
         .def("calculate_pair_correlations", [](MDDriver &d) { d.pair_correlation(1); })
         .def("calculate_partial_pair_correlation", [](MDDriver &d) { d.pair_correlation(2); })
+        .def("set_sample_ring", &MDDriver::set_sample_ring, py::arg("capacity"),
+             "room for this many sampled steps between drains (0: no ring)")
+        .def("drain_samples", &MDDriver::drain_samples,
+             "records of the sampled steps since the last drain, as arrays")
+        .def("fluctuation_start", &MDDriver::fluctuation_start,
+             "clear the fluctuation sums and accumulate from the next sampled step")
+        .def("fluctuations", &MDDriver::fluctuations)
+        .def("elastic_constants", &MDDriver::elastic_constants, py::arg("T") = py::none(),
+             py::arg("P") = py::none(),
+             "the fluctuation estimate of C_ij from the accumulated sums (defaults: the "
+             "thermostat temperature and barostat pressure)")
         // additions of the B200 path
         .def("integrate_n", &MDDriver::integrate_n, py::arg("n_steps"))
         .def("atoms_array", &MDDriver::atoms_array, py::arg("field"))
@@ -819,6 +964,12 @@ PYBIND11_MODULE(md_driver_module, m) {
         .def("observables", &BatchedMDDriver::observables, py::arg("replica"))
         .def("atoms", &BatchedMDDriver::atoms, py::arg("replica"), py::arg("field"))
         .def("kernel_times", &BatchedMDDriver::kernel_times, py::arg("n_steps") = 10)
+        .def("set_sample_ring", &BatchedMDDriver::set_sample_ring, py::arg("capacity"))
+        .def("drain_samples", &BatchedMDDriver::drain_samples, py::arg("replica"))
+        .def("fluctuation_start", &BatchedMDDriver::fluctuation_start)
+        .def("fluctuations", &BatchedMDDriver::fluctuations, py::arg("replica"))
+        .def("elastic_constants", &BatchedMDDriver::elastic_constants, py::arg("replica"),
+             py::arg("T") = py::none(), py::arg("P") = py::none())
         .def("pair_correlation", &BatchedMDDriver::pair_correlation, py::arg("replica"),
              py::arg("mode") = 1)
         .def("synchronize", &BatchedMDDriver::synchronize);

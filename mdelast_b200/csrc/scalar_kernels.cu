@@ -351,6 +351,90 @@ __global__ void k_reduce(AtomsView A) {
             (part[0][q] + part[1][q]) + (part[2][q] + part[3][q]);
 }
 
+// One sampled step: append what molecular_dynamics.py:1218-1238 reads to the replica's
+// ring, and, while accumulating, fold x = (sigma^B[6], N/V, V, etot_atom) and C^B into the
+// running means and co-moments (Welford's updates; the production-window sums behind
+// molecular_dynamics.py:776-958).
+__device__ void record_sample(AtomsView const &A, int r, Replica *R, double V) {
+    mdelast_observables const &o = R->obs;
+    if (A.ring && A.ring_cap > 0) {
+        long const slot = static_cast<long>(R->n_samples) % A.ring_cap;
+        mdelast_sample &s = A.ring[static_cast<size_t>(r) * A.ring_cap + slot];
+        s.time = o.time;
+        s.cycle = o.cycle;
+        s.temperature_kin = o.temperature_kin;
+        s.temperature_conf_inverse = o.temperature_conf_inverse;
+        s.total_laplacian = o.total_laplacian;
+        s.total_force2 = o.total_force2;
+        s.pressure = o.pressure;
+        for (int k = 0; k < 6; ++k) {
+            s.stress_tensor[k] = o.stress_tensor[k];
+            s.born_stress_tensor[k] = o.born_stress_tensor[k];
+        }
+        s.etot_atom = o.etot_atom;
+        s.epot_atom = o.epot_atom;
+        s.epot_eam_atom = o.epot_eam_atom;
+        s.ekin_atom = o.ekin_atom;
+        s.etot_cons = o.etot_cons;
+        s.etot_cons_err = o.etot_cons_err;
+        int q = 0;
+        for (int a = 0; a < 6; ++a)
+            for (int b = a; b < 6; ++b, ++q)
+                s.born_elasticity_tensor[q] = o.born_elasticity_tensor[6 * a + b];
+        s.volume = V;
+        s.status = static_cast<double>(o.status);
+        R->n_samples += 1.;
+    }
+    if (!R->acc_on)
+        return;
+    mdelast_fluct &f = R->acc;
+    double x[9];
+    for (int k = 0; k < 6; ++k)
+        x[k] = o.born_stress_tensor[k];
+    x[6] = R->n_atoms / V;
+    x[7] = V;
+    x[8] = o.etot_atom;
+    f.n += 1.;
+    double const inv_n = 1. / f.n;
+    double d0[9], d1[9];
+    for (int k = 0; k < 9; ++k) {
+        d0[k] = x[k] - f.mean[k];
+        f.mean[k] += d0[k] * inv_n;
+        d1[k] = x[k] - f.mean[k];
+    }
+    int q = 0;
+    for (int a = 0; a < 9; ++a)
+        for (int b = a; b < 9; ++b, ++q)
+            f.comoment[q] += d0[a] * d1[b];
+    q = 0;
+    for (int a = 0; a < 6; ++a)
+        for (int b = a; b < 6; ++b, ++q)
+            f.born_el_mean[q] += (o.born_elasticity_tensor[6 * a + b] - f.born_el_mean[q]) * inv_n;
+}
+
+// what & 1: empty every replica's sample ring; what & 2: clear the fluctuation sums and
+// start accumulating.
+__global__ void k_samples_reset(AtomsView A, int what) {
+    int const r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= A.n_rep)
+        return;
+    Replica *R = A.rep + r;
+    if (what & 1)
+        R->n_samples = 0.;
+    if (what & 2) {
+        mdelast_fluct &f = R->acc;
+        f.n = 0.;
+        f.n_atoms = R->n_atoms;
+        for (int k = 0; k < 9; ++k)
+            f.mean[k] = 0.;
+        for (int k = 0; k < 45; ++k)
+            f.comoment[k] = 0.;
+        for (int k = 0; k < 21; ++k)
+            f.born_el_mean[k] = 0.;
+        R->acc_on = 1;
+    }
+}
+
 __global__ void k_post(AtomsView A, int mode, int obs) {
     Replica *R = A.rep + blockIdx.x;
     __shared__ double sf[F_NSUM], sd[D_NSUM];
@@ -509,6 +593,8 @@ __global__ void k_post(AtomsView A, int mode, int obs) {
     o.baro_epsilon = R->eps;
     o.baro_p_epsilon = R->p_eps;
     o.sample_observables = obs;
+    if (mode == POST_STEP && obs)
+        record_sample(A, static_cast<int>(blockIdx.x), R, V);
 }
 
 } // namespace mdelast
