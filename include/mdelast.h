@@ -268,6 +268,20 @@ int mdelast_driver_get_gr(mdelast_driver *d, double *gr, double *gr_partial);
 int mdelast_batch_pair_correlation(mdelast_driver *d, int32_t replica, int32_t mode);
 int mdelast_batch_get_gr(mdelast_driver *d, int32_t replica, double *gr, double *gr_partial);
 
+/* Launch shapes of the two pair passes. No counterpart in the reference (its loops are
+ * serial). autotune times the density and the force pass (sampled-step variants when the
+ * driver samples observables, else the plain ones) on the current positions for every
+ * lanes-per-atom value in {1, 4, 8, 16} and block target in {8, 16, 32, 64} x 148, n_repeat
+ * launches each, keeps the fastest for each pass and recomputes the per-atom state with it;
+ * the state does not advance. choice (4 values, may be NULL): lanes per atom of the density
+ * and force passes, block targets of the density and force passes; ms_out (2, may be NULL):
+ * their mean times in ms. set_launch sets a shape directly. Both drop the captured step
+ * graphs (recaptured on the next step). */
+int mdelast_driver_autotune(mdelast_driver *d, int32_t n_repeat, int32_t *choice,
+                            double *ms_out);
+int mdelast_driver_set_launch(mdelast_driver *d, int32_t tpa_density, int32_t tpa_force,
+                              int32_t blocks_density, int32_t blocks_force);
+
 /* ---- Samples and fluctuation sums (molecular_dynamics.py:1218-1238, 663-1000) ----
  *
  * Every step that samples observables (sample_observables set, or the sampled steps of

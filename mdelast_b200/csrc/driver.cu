@@ -60,14 +60,14 @@ int default_tpa(int n_atoms) {
 }
 
 // Deal the blocks of a pair pass out to the replicas in proportion to their atom counts:
-// at most kTargetBlocks in all (many resident waves on 148 SMs: a block then loops over
-// several atom groups only for large batches), never fewer than one per replica nor more
-// than one per atom group of kBlock/tpa atoms. Fills each replica's block range and the
-// block -> replica map; returns the grid size.
+// about `target` in all (a multiple of the 148 SMs: a block then loops over several atom
+// groups only for large batches), never fewer than one per replica nor more than one per
+// atom group of kBlock/tpa atoms. Fills each replica's block range and the block ->
+// replica map; returns the grid size.
 constexpr int kTargetBlocks = 148 * 32;
 
 int deal_blocks(std::vector<Replica *> const &reps, int tpa, bool density,
-                std::vector<int> &blk_rep) {
+                std::vector<int> &blk_rep, int target = kTargetBlocks) {
     long total = 0;
     for (Replica const *r : reps)
         total += r->n_blocks;
@@ -75,7 +75,7 @@ int deal_blocks(std::vector<Replica *> const &reps, int tpa, bool density,
     for (size_t k = 0; k < reps.size(); ++k) {
         Replica *r = reps[k];
         long const most = static_cast<long>(r->n_blocks) * tpa;
-        long nb = (static_cast<long>(kTargetBlocks) * r->n_blocks + total - 1) / total;
+        long nb = (static_cast<long>(target) * r->n_blocks + total - 1) / total;
         nb = std::max(1L, std::min(nb, most));
         if (density) {
             r->dblk_begin = static_cast<int>(blk_rep.size());
@@ -194,6 +194,10 @@ struct mdelast_driver_s {
     int launch_steps(int n_steps, int rebuild_every, int sample_every);
     int wait_step();
     int check_status();
+    // launch shape of the pair passes: lanes per atom and target block counts
+    int target_d = kTargetBlocks, target_f = kTargetBlocks;
+    int set_launch(int tpa_d_, int tpa_f_, int tgt_d, int tgt_f);
+    int time_passes(int n_repeat, int obs, double *ms_d, double *ms_f);
 };
 
 mdelast_driver_s::~mdelast_driver_s() {
@@ -266,6 +270,90 @@ int mdelast_driver_s::alloc_cells(int n_cells, int cell_cap) {
     cells_alloc = n_cells;
     A.cell_cap = cell_cap;
     drop_graphs();
+    return MDELAST_OK;
+}
+
+// Re-deal the pair-pass blocks for new lanes-per-atom and block targets: replica block
+// ranges, block -> replica maps, per-block and per-chunk partial-sum buffers. The step
+// graphs hold the old shapes and are dropped. Call with no work in flight.
+int mdelast_driver_s::set_launch(int tpa_d_, int tpa_f_, int tgt_d, int tgt_f) {
+    if (!valid_tpa(tpa_d_) || !valid_tpa(tpa_f_) || tgt_d < 1 || tgt_f < 1)
+        return fail(MDELAST_ERR_ARGUMENT, "bad launch shape");
+    CK(cudaStreamSynchronize(stream));
+    std::vector<Replica> R(static_cast<size_t>(n_rep));
+    CK(cudaMemcpy(R.data(), d_rep, sizeof(Replica) * n_rep, cudaMemcpyDeviceToHost));
+    std::vector<Replica *> reps;
+    for (auto &x : R)
+        reps.push_back(&x);
+    std::vector<int> dmap, fmap;
+    int const gd = deal_blocks(reps, tpa_d_, true, dmap, tgt_d);
+    int const gf = deal_blocks(reps, tpa_f_, false, fmap, tgt_f);
+    int chunks = 1;
+    for (Replica const *x : reps)
+        chunks = std::max(chunks, (std::max(x->dblk_n, x->fblk_n) + kChunk - 1) / kChunk);
+    drop_graphs();
+    dfree(d_dblk_rep);
+    dfree(d_fblk_rep);
+    dfree(d_pd);
+    dfree(d_pf);
+    dfree(d_red);
+    if (int rc = dalloc(&d_dblk_rep, dmap.size()))
+        return rc;
+    if (int rc = dalloc(&d_fblk_rep, fmap.size()))
+        return rc;
+    if (int rc = dalloc(&d_pd, static_cast<size_t>(gd) * D_NSUM))
+        return rc;
+    if (int rc = dalloc(&d_pf, static_cast<size_t>(gf) * F_NSUM))
+        return rc;
+    if (int rc = dalloc(&d_red, static_cast<size_t>(n_rep) * chunks * 64))
+        return rc;
+    CK(cudaMemcpy(d_dblk_rep, dmap.data(), sizeof(int) * dmap.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_fblk_rep, fmap.data(), sizeof(int) * fmap.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_rep, R.data(), sizeof(Replica) * n_rep, cudaMemcpyHostToDevice));
+    tpa_d = tpa_d_;
+    tpa_f = tpa_f_;
+    target_d = tgt_d;
+    target_f = tgt_f;
+    grid_d = gd;
+    grid_f = gf;
+    A.dblk_rep = d_dblk_rep;
+    A.fblk_rep = d_fblk_rep;
+    A.pd = d_pd;
+    A.pf = d_pf;
+    A.red = d_red;
+    A.max_chunks = chunks;
+    return MDELAST_OK;
+}
+
+// Mean device time of the density and the force pass (no kick: the state is unchanged)
+// over n_repeat launches on the current positions, after one untimed pair.
+int mdelast_driver_s::time_passes(int n_repeat, int obs, double *ms_d, double *ms_f) {
+    cudaEvent_t ev[3];
+    for (auto &e : ev)
+        CK(cudaEventCreate(&e));
+    double td = 0., tf = 0.;
+    cudaError_t err = cudaSuccess;
+    for (int k = 0; k <= n_repeat && err == cudaSuccess; ++k) {
+        cudaEventRecord(ev[0], stream);
+        pass_density(obs != 0, stream);
+        cudaEventRecord(ev[1], stream);
+        pass_force(obs != 0, false, stream);
+        cudaEventRecord(ev[2], stream);
+        err = cudaEventSynchronize(ev[2]);
+        if (err == cudaSuccess && k > 0) {
+            float a = 0.f, b = 0.f;
+            cudaEventElapsedTime(&a, ev[0], ev[1]);
+            cudaEventElapsedTime(&b, ev[1], ev[2]);
+            td += a;
+            tf += b;
+        }
+    }
+    for (auto &e : ev)
+        cudaEventDestroy(e);
+    if (err != cudaSuccess)
+        return fail(MDELAST_ERR_CUDA, "pass timing: %s", cudaGetErrorString(err));
+    *ms_d = td / n_repeat;
+    *ms_f = tf / n_repeat;
     return MDELAST_OK;
 }
 
@@ -1254,6 +1342,69 @@ static int get_fluct_r(mdelast_driver *d, int r, mdelast_fluct *out) {
 }
 
 extern "C" {
+
+int mdelast_driver_autotune(mdelast_driver *d, int32_t n_repeat, int32_t *choice,
+                            double *ms_out) {
+    clear_error();
+    if (!d || n_repeat < 1)
+        return fail(MDELAST_ERR_ARGUMENT, "bad argument");
+    CK(cudaSetDevice(d->device));
+    if (int rc = d->wait_step())
+        return rc;
+    int const tpas[4] = {1, 4, 8, 16};
+    int const targets[4] = {148 * 8, 148 * 16, 148 * 32, 148 * 64};
+    double best_d = 1e300, best_f = 1e300;
+    int bd[2] = {d->tpa_d, d->target_d}, bf[2] = {d->tpa_f, d->target_f};
+    for (int tp : tpas)
+        for (int tg : targets) {
+            if (int rc = d->set_launch(tp, tp, tg, tg))
+                return rc;
+            double md = 0., mf = 0.;
+            if (int rc = d->time_passes(n_repeat, d->sample, &md, &mf))
+                return rc;
+            if (md < best_d) {
+                best_d = md;
+                bd[0] = tp;
+                bd[1] = tg;
+            }
+            if (mf < best_f) {
+                best_f = mf;
+                bf[0] = tp;
+                bf[1] = tg;
+            }
+        }
+    if (int rc = d->set_launch(bd[0], bf[0], bd[1], bf[1]))
+        return rc;
+    // recompute the per-atom state with the chosen shapes (positions are unchanged)
+    double md = 0., mf = 0.;
+    if (int rc = d->time_passes(1, 1, &md, &mf))
+        return rc;
+    if (choice) {
+        choice[0] = bd[0];
+        choice[1] = bf[0];
+        choice[2] = bd[1];
+        choice[3] = bf[1];
+    }
+    if (ms_out) {
+        ms_out[0] = best_d;
+        ms_out[1] = best_f;
+    }
+    return MDELAST_OK;
+}
+
+int mdelast_driver_set_launch(mdelast_driver *d, int32_t tpa_density, int32_t tpa_force,
+                              int32_t blocks_density, int32_t blocks_force) {
+    clear_error();
+    if (!d)
+        return fail(MDELAST_ERR_ARGUMENT, "null driver");
+    CK(cudaSetDevice(d->device));
+    if (int rc = d->wait_step())
+        return rc;
+    if (int rc = d->set_launch(tpa_density, tpa_force, blocks_density, blocks_force))
+        return rc;
+    double md = 0., mf = 0.;
+    return d->time_passes(1, 1, &md, &mf);
+}
 
 int mdelast_driver_set_sample_ring(mdelast_driver *d, int32_t capacity) {
     clear_error();

@@ -140,6 +140,20 @@ py::dict elastic_dict(mdelast_fluct const &f, int ensemble, double T, double P) 
     return out;
 }
 
+py::dict autotune_dict(mdelast_driver *d, int n_repeat) {
+    int32_t c[4];
+    double ms[2];
+    check(mdelast_driver_autotune(d, n_repeat, c, ms));
+    py::dict out;
+    out["tpa_density"] = c[0];
+    out["tpa_force"] = c[1];
+    out["blocks_density"] = c[2];
+    out["blocks_force"] = c[3];
+    out["ms_density"] = ms[0];
+    out["ms_force"] = ms[1];
+    return out;
+}
+
 int parse_interp(std::string const &name) {
     if (name == "quintic")
         return MDELAST_QUINTIC;
@@ -531,6 +545,10 @@ class MDDriver {
     }
     void synchronize() { check(mdelast_driver_synchronize(d_)); }
     void set_sample_ring(int capacity) { check(mdelast_driver_set_sample_ring(d_, capacity)); }
+    py::dict autotune(int n_repeat) { return autotune_dict(d_, n_repeat); }
+    void set_launch(int td, int tf, int bd, int bf) {
+        check(mdelast_driver_set_launch(d_, td, tf, bd, bf));
+    }
     py::dict drain_samples() { return drain_dict(d_, -1); }
     void fluctuation_start() { check(mdelast_driver_fluct_start(d_)); }
     mdelast_fluct fluct() {
@@ -741,6 +759,10 @@ class BatchedMDDriver {
     // g(r) of one replica (mode as MDDriver's three calculate_* methods: 0, 1, 2);
     // returns (gr, gr_partial) with gr_partial one row per type pair a <= b
     void set_sample_ring(int capacity) { check(mdelast_driver_set_sample_ring(d_, capacity)); }
+    py::dict autotune(int n_repeat) { return autotune_dict(d_, n_repeat); }
+    void set_launch(int td, int tf, int bd, int bf) {
+        check(mdelast_driver_set_launch(d_, td, tf, bd, bf));
+    }
     py::dict drain_samples(int r) {
         if (r < 0 || r >= n_replicas())
             throw py::index_error("replica index out of range");
@@ -911,6 +933,10 @@ PYBIND11_MODULE(md_driver_module, m) {
         .def("calculate_pair_correlation", [](MDDriver &d) { d.pair_correlation(0); })
         .def("calculate_pair_correlations", [](MDDriver &d) { d.pair_correlation(1); })
         .def("calculate_partial_pair_correlation", [](MDDriver &d) { d.pair_correlation(2); })
+        .def("autotune", &MDDriver::autotune, py::arg("n_repeat") = 3,
+             "time the pair passes over their launch shapes and keep the fastest")
+        .def("set_launch", &MDDriver::set_launch, py::arg("tpa_density"), py::arg("tpa_force"),
+             py::arg("blocks_density"), py::arg("blocks_force"))
         .def("set_sample_ring", &MDDriver::set_sample_ring, py::arg("capacity"),
              "room for this many sampled steps between drains (0: no ring)")
         .def("drain_samples", &MDDriver::drain_samples,
@@ -964,6 +990,9 @@ PYBIND11_MODULE(md_driver_module, m) {
         .def("observables", &BatchedMDDriver::observables, py::arg("replica"))
         .def("atoms", &BatchedMDDriver::atoms, py::arg("replica"), py::arg("field"))
         .def("kernel_times", &BatchedMDDriver::kernel_times, py::arg("n_steps") = 10)
+        .def("autotune", &BatchedMDDriver::autotune, py::arg("n_repeat") = 3)
+        .def("set_launch", &BatchedMDDriver::set_launch, py::arg("tpa_density"),
+             py::arg("tpa_force"), py::arg("blocks_density"), py::arg("blocks_force"))
         .def("set_sample_ring", &BatchedMDDriver::set_sample_ring, py::arg("capacity"))
         .def("drain_samples", &BatchedMDDriver::drain_samples, py::arg("replica"))
         .def("fluctuation_start", &BatchedMDDriver::fluctuation_start)

@@ -24,7 +24,7 @@ __device__ __forceinline__ int tab_locate_f(float x, float inv_h, int n, float &
         i = n - 1;
     else if (u > 0.f)
         i = static_cast<int>(u);
-    t = u - static_cast<float>(i);
+    t = __fsub_rn(u, static_cast<float>(i));
     return i;
 }
 
@@ -39,11 +39,19 @@ __device__ __forceinline__ void ld6f(const float *p, float c[6]) {
     c[5] = d.y;
 }
 
+// The pair force is evaluated from both of its atoms, in different code paths of the
+// force pass; its arithmetic is written with explicit rounding (no contraction left to
+// the compiler) so that both evaluations give the same bits.
 __device__ __forceinline__ float tabf_v(const float *c, float t) {
     return c[0] + t * (c[1] + t * (c[2] + t * (c[3] + t * (c[4] + t * c[5]))));
 }
 __device__ __forceinline__ float tabf_d1(const float *c, float t, float inv_h) {
-    return (c[1] + t * (2.f * c[2] + t * (3.f * c[3] + t * (4.f * c[4] + t * 5.f * c[5])))) * inv_h;
+    float p = __fmul_rn(5.f, c[5]);
+    p = __fmaf_rn(t, p, __fmul_rn(4.f, c[4]));
+    p = __fmaf_rn(t, p, __fmul_rn(3.f, c[3]));
+    p = __fmaf_rn(t, p, __fmul_rn(2.f, c[2]));
+    p = __fmaf_rn(t, p, c[1]);
+    return __fmul_rn(p, inv_h);
 }
 __device__ __forceinline__ float tabf_d2(const float *c, float t, float inv_h2) {
     return (2.f * c[2] + t * (6.f * c[3] + t * (12.f * c[4] + t * 20.f * c[5]))) * inv_h2;
@@ -52,13 +60,13 @@ __device__ __forceinline__ float tabf_d2(const float *c, float t, float inv_h2) 
 // minimum image of pi - pj in a box of edges L (positions wrapped into [-L/2, L/2))
 __device__ __forceinline__ float min_image_f(float4 pi, float4 pj, float3 L, float3 iL,
                                              float &dx, float &dy, float &dz) {
-    dx = pi.x - pj.x;
-    dy = pi.y - pj.y;
-    dz = pi.z - pj.z;
-    dx -= L.x * rintf(dx * iL.x);
-    dy -= L.y * rintf(dy * iL.y);
-    dz -= L.z * rintf(dz * iL.z);
-    return dx * dx + dy * dy + dz * dz;
+    dx = __fsub_rn(pi.x, pj.x);
+    dy = __fsub_rn(pi.y, pj.y);
+    dz = __fsub_rn(pi.z, pj.z);
+    dx = __fmaf_rn(-L.x, rintf(__fmul_rn(dx, iL.x)), dx);
+    dy = __fmaf_rn(-L.y, rintf(__fmul_rn(dy, iL.y)), dy);
+    dz = __fmaf_rn(-L.z, rintf(__fmul_rn(dz, iL.z)), dz);
+    return __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
 }
 
 __device__ __forceinline__ void box_f(Replica const *R, float3 &L, float3 &iL) {
@@ -88,6 +96,10 @@ __global__ void k_posf(AtomsView A) {
 // Density pass of md_driver.cpp:195-277 in mixed precision (see k_density for the roles).
 template <bool OBS, int TPA>
 __global__ void __launch_bounds__(kBlock) k_density_mx(AtomsView A, TablesView T) {
+    double acc[D_NSUM];
+#pragma unroll
+    for (int k = 0; k < D_NSUM; ++k)
+        acc[k] = 0.;
     int const r = A.dblk_rep[blockIdx.x];
     Replica const *R = A.rep + r;
     int const lb = blockIdx.x - R->dblk_begin, nb = R->dblk_n;
@@ -95,10 +107,6 @@ __global__ void __launch_bounds__(kBlock) k_density_mx(AtomsView A, TablesView T
     int const n_slots = R->n_blocks * kBlock;
     float3 L, iL;
     box_f(R, L, iL);
-    double acc[D_NSUM];
-#pragma unroll
-    for (int k = 0; k < D_NSUM; ++k)
-        acc[k] = 0.;
     for (int a0 = lb * apb; a0 < n_slots; a0 += nb * apb) {
         int const a = a0 + static_cast<int>(threadIdx.x) / TPA;
         int const i = R->atom_begin + a;
@@ -200,141 +208,199 @@ __global__ void __launch_bounds__(kBlock) k_density_mx(AtomsView A, TablesView T
     block_sum_store<D_NSUM>(acc, A.pd + static_cast<size_t>(blockIdx.x) * D_NSUM);
 }
 
+// Sums over the pairs of one lane's share of an atom row, added into the FP64 block
+// accumulators once per row. The virial and the diagonal Born stress are summed in FP64
+// pair by pair (the reference checks the virial against the stress trace to 1e-7,
+// md_driver.cpp:422-429); the off-diagonal stress, Born tensor and Laplacian terms are
+// summed in FP32 along the row (at most ~20 FP32 terms, no error beyond the terms' own)
+// and in FP64 across rows and atoms.
+template <bool OBS> struct PairSums {
+    double vir = 0., sig_d[3] = {0., 0., 0.};
+    float sig_o[3] = {0, 0, 0};
+    float cb[OBS ? 15 : 1] = {};
+    float lap = 0.f;
+};
+
+// Per-atom inputs of one row of the force pass.
+struct RowIn {
+    float4 pi;
+    float dFi, d2Fi;
+    int ti;
+    float3 L, iL;
+};
+
+// One lane's walk over list slots [s0, s1) of an atom row (slots of partners j > i when
+// UPPER, else of partners j < i, addressed from the end of the row); every pair adds its
+// force and half its energy to the atom, and pairs j > i also add to the global sums.
+template <bool OBS, bool UPPER, int TPA>
+__device__ __forceinline__ void force_row_mx(AtomsView const &A, TablesView const &T,
+                                             RowIn const &in, const int *row, int n, int sub,
+                                             double &fx, double &fy, double &fz, double &epot,
+                                             PairSums<OBS> &ps, bool &warn_rmin) {
+    if (sub >= n)
+        return;
+    auto slot = [&](int k) { return UPPER ? k : A.maxn - 1 - k; };
+    int jn = row[slot(sub)];
+    float4 pn = A.posf[jn];
+    float2 fn = A.dF2f[jn];
+    for (int kk = sub; kk < n; kk += TPA) {
+        float4 const pj = pn;
+        float2 const dFj2 = fn;
+        if (kk + TPA < n) {
+            jn = row[slot(kk + TPA)];
+            pn = A.posf[jn];
+            fn = A.dF2f[jn];
+        }
+        float dx, dy, dz;
+        float const r2 = min_image_f(in.pi, pj, in.L, in.iL, dx, dy, dz);
+        if (r2 > T.fr_cut_sq)
+            continue;
+        float const idr = rsqrtf(r2);
+        float const dr = __fmul_rn(r2, idr);
+        int const tj = static_cast<int>(pj.w);
+        int const ti = in.ti;
+        int const s = pair_slot(ti, tj);
+        float t;
+        int const k = tab_locate_f(dr, T.finv_hr, T.nri, t);
+        const float *bundle = T.rbf + (static_cast<size_t>(s) * T.nri + k) * 18;
+        float V = 0.f, dV = 0.f, d2V = 0.f;
+        if (dr < T.fpot_rmin[s])
+            warn_rmin = true;
+        if (!(dr > T.fpot_rcut[s])) {
+            float c[6];
+            ld6f(bundle, c);
+            V = tabf_v(c, t);
+            dV = tabf_d1(c, t, T.finv_hr);
+            if (OBS)
+                d2V = tabf_d2(c, t, T.finv_hr2);
+        }
+        float dedr = dV, X = 0.f, lap = 0.f;
+        if (OBS) {
+            X = d2V - dV * idr;
+            lap = 2.f * (d2V + 2.f * dV * idr);
+        }
+        if (T.has_eam) {
+            int const oi = (ti <= tj) ? 6 : 12, oj = (ti < tj) ? 12 : 6;
+            float drho_i = 0.f, drho_j = 0.f, d2rho_i = 0.f, d2rho_j = 0.f;
+            if (!(dr > T.feam_rcut[ti])) {
+                float c[6];
+                ld6f(bundle + oi, c);
+                drho_i = tabf_d1(c, t, T.finv_hr);
+                if (OBS)
+                    d2rho_i = tabf_d2(c, t, T.finv_hr2);
+            }
+            if (!(dr > T.feam_rcut[tj])) {
+                float c[6];
+                ld6f(bundle + oj, c);
+                drho_j = tabf_d1(c, t, T.finv_hr);
+                if (OBS)
+                    d2rho_j = tabf_d2(c, t, T.finv_hr2);
+            }
+            float const dFj = dFj2.x, dFi = in.dFi;
+            // the two cross terms rounded separately and added commutatively: the pair
+            // force is the same, bit for bit, seen from either atom
+            dedr = __fadd_rn(dedr, __fadd_rn(__fmul_rn(dFi, drho_j), __fmul_rn(dFj, drho_i)));
+            if (OBS && UPPER) {
+                float const d2Fj = dFj2.y, d2Fi = in.d2Fi;
+                lap += 2.f * (dFj * (d2rho_i + 2.f * drho_i * idr) +
+                              dFi * (d2rho_j + 2.f * drho_j * idr));
+                lap += d2Fi * (drho_j * drho_j) + d2Fj * (drho_i * drho_i);
+                X += dFi * (d2rho_j - drho_j * idr) + dFj * (d2rho_i - drho_i * idr);
+            }
+        }
+        float const sc = __fmul_rn(-dedr, idr);
+        fx += static_cast<double>(__fmul_rn(sc, dx));
+        fy += static_cast<double>(__fmul_rn(sc, dy));
+        fz += static_cast<double>(__fmul_rn(sc, dz));
+        epot += static_cast<double>(0.5f * V);
+        if (UPPER) {
+            ps.vir += static_cast<double>(dr * dedr);
+            float const xx = dx * dx, yy = dy * dy, zz = dz * dz;
+            float const yz = dy * dz, xz = dx * dz, xy = dx * dy;
+            float const w = dedr * idr;
+            ps.sig_d[0] += static_cast<double>(w * xx);
+            ps.sig_d[1] += static_cast<double>(w * yy);
+            ps.sig_d[2] += static_cast<double>(w * zz);
+            ps.sig_o[0] += w * yz;
+            ps.sig_o[1] += w * xz;
+            ps.sig_o[2] += w * xy;
+            if (OBS) {
+                X *= idr * idr;
+                float const Xxx = X * xx, Xyy = X * yy, Xzz = X * zz;
+                ps.cb[0] += Xxx * xx;
+                ps.cb[1] += Xyy * yy;
+                ps.cb[2] += Xzz * zz;
+                ps.cb[3] += Xxx * xy;
+                ps.cb[4] += Xxx * xz;
+                ps.cb[5] += Xyy * xy;
+                ps.cb[6] += Xyy * yz;
+                ps.cb[7] += Xzz * xz;
+                ps.cb[8] += Xzz * yz;
+                ps.cb[9] += Xxx * yy;
+                ps.cb[10] += Xxx * zz;
+                ps.cb[11] += Xyy * zz;
+                ps.cb[12] += Xxx * yz;
+                ps.cb[13] += Xyy * xz;
+                ps.cb[14] += Xzz * xy;
+                ps.lap += lap;
+            }
+        }
+    }
+}
+
 // Force pass of md_driver.cpp:300-430 (with the closing kick) in mixed precision; see
-// k_force for the roles of the terms.
+// k_force for the roles of the terms. Each atom row is walked in two loops, partners j > i
+// (which also feed the global sums) and partners j < i, so the lanes of a warp do not
+// diverge on the global-sum work. The per-thread FP64 block accumulators live in shared
+// memory (slot-major) rather than registers.
 template <bool OBS, bool KICK, int TPA>
 __global__ void __launch_bounds__(kBlock) k_force_mx(AtomsView A, TablesView T) {
+    __shared__ double s_acc[F_NSUM * kBlock];
+    int const tid = threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < F_NSUM; ++k)
+        s_acc[k * kBlock + tid] = 0.;
     int const r = A.fblk_rep[blockIdx.x];
     Replica const *R = A.rep + r;
     int const lb = blockIdx.x - R->fblk_begin, nb = R->fblk_n;
-    int const apb = kBlock / TPA, sub = threadIdx.x % TPA;
+    int const apb = kBlock / TPA, sub = tid % TPA;
     int const n_slots = R->n_blocks * kBlock;
-    float3 L, iL;
-    box_f(R, L, iL);
-    double acc[F_NSUM];
-#pragma unroll
-    for (int k = 0; k < F_NSUM; ++k)
-        acc[k] = 0.;
+    RowIn in;
+    box_f(R, in.L, in.iL);
     for (int a0 = lb * apb; a0 < n_slots; a0 += nb * apb) {
-        int const a = a0 + static_cast<int>(threadIdx.x) / TPA;
+        int const a = a0 + tid / TPA;
         int const i = R->atom_begin + a;
         bool const valid = a < R->n_atoms;
         double fx = 0., fy = 0., fz = 0., epot = 0.;
-        int ti = 0;
+        in.ti = 0;
         if (valid) {
-            float4 const pi = A.posf[i];
-            ti = static_cast<int>(pi.w);
+            in.pi = A.posf[i];
+            in.ti = static_cast<int>(in.pi.w);
             float2 const dFi2 = T.has_eam ? A.dF2f[i] : make_float2(0.f, 0.f);
-            float const dFi = dFi2.x, d2Fi = OBS ? dFi2.y : 0.f;
-            int const nu = A.n_up[i], ntot = nu + A.n_dn[i];
+            in.dFi = dFi2.x;
+            in.d2Fi = OBS ? dFi2.y : 0.f;
+            int const nu = A.n_up[i], nd = A.n_dn[i];
             int const *row = A.nbr + static_cast<size_t>(i) * A.maxn;
             bool warn_rmin = false;
-            int jn = sub < ntot ? row[list_slot(sub, nu, A.maxn)] : i;
-            float4 pn = A.posf[jn];
-            float2 fn = A.dF2f[jn];
-            for (int kk = sub; kk < ntot; kk += TPA) {
-                bool const upper = kk < nu;
-                float4 const pj = pn;
-                float2 const dFj2 = fn;
-                if (kk + TPA < ntot) {
-                    jn = row[list_slot(kk + TPA, nu, A.maxn)];
-                    pn = A.posf[jn];
-                    fn = A.dF2f[jn];
-                }
-                float dx, dy, dz;
-                float const r2 = min_image_f(pi, pj, L, iL, dx, dy, dz);
-                if (r2 > T.fr_cut_sq)
-                    continue;
-                float const dr = sqrtf(r2);
-                float const idr = 1.f / dr;
-                int const tj = static_cast<int>(pj.w);
-                int const s = pair_slot(ti, tj);
-                float t;
-                int const k = tab_locate_f(dr, T.finv_hr, T.nri, t);
-                const float *bundle = T.rbf + (static_cast<size_t>(s) * T.nri + k) * 18;
-                float V = 0.f, dV = 0.f, d2V = 0.f;
-                if (dr < T.fpot_rmin[s])
-                    warn_rmin = true;
-                if (!(dr > T.fpot_rcut[s])) {
-                    float c[6];
-                    ld6f(bundle, c);
-                    V = tabf_v(c, t);
-                    dV = tabf_d1(c, t, T.finv_hr);
-                    if (OBS)
-                        d2V = tabf_d2(c, t, T.finv_hr2);
-                }
-                float dedr = dV, X = 0.f, lap = 0.f;
-                if (OBS) {
-                    X = d2V - dV * idr;
-                    lap = 2.f * (d2V + 2.f * dV * idr);
-                }
-                if (T.has_eam) {
-                    int const oi = (ti <= tj) ? 6 : 12, oj = (ti < tj) ? 12 : 6;
-                    float drho_i = 0.f, drho_j = 0.f, d2rho_i = 0.f, d2rho_j = 0.f;
-                    if (!(dr > T.feam_rcut[ti])) {
-                        float c[6];
-                        ld6f(bundle + oi, c);
-                        drho_i = tabf_d1(c, t, T.finv_hr);
-                        if (OBS)
-                            d2rho_i = tabf_d2(c, t, T.finv_hr2);
-                    }
-                    if (!(dr > T.feam_rcut[tj])) {
-                        float c[6];
-                        ld6f(bundle + oj, c);
-                        drho_j = tabf_d1(c, t, T.finv_hr);
-                        if (OBS)
-                            d2rho_j = tabf_d2(c, t, T.finv_hr2);
-                    }
-                    float const dFj = dFj2.x;
-                    dedr = __fadd_rn(dedr, __fadd_rn(__fmul_rn(dFi, drho_j), __fmul_rn(dFj, drho_i)));
-                    if (OBS) {
-                        float const d2Fj = dFj2.y;
-                        lap += 2.f * (dFj * (d2rho_i + 2.f * drho_i * idr) +
-                                      dFi * (d2rho_j + 2.f * drho_j * idr));
-                        lap += d2Fi * (drho_j * drho_j) + d2Fj * (drho_i * drho_i);
-                        X += dFi * (d2rho_j - drho_j * idr) + dFj * (d2rho_i - drho_i * idr);
-                    }
-                }
-                float const sc = __fmul_rn(-dedr, idr);
-                fx += static_cast<double>(__fmul_rn(sc, dx));
-                fy += static_cast<double>(__fmul_rn(sc, dy));
-                fz += static_cast<double>(__fmul_rn(sc, dz));
-                epot += static_cast<double>(0.5f * V);
-                if (upper) {
-                    acc[F_VIRIAL] += static_cast<double>(dr * dedr);
-                    float const xx = dx * dx, yy = dy * dy, zz = dz * dz;
-                    float const yz = dy * dz, xz = dx * dz, xy = dx * dy;
-                    float const w = dedr * idr;
-                    acc[F_SIGMA + 0] += static_cast<double>(w * xx);
-                    acc[F_SIGMA + 1] += static_cast<double>(w * yy);
-                    acc[F_SIGMA + 2] += static_cast<double>(w * zz);
-                    acc[F_SIGMA + 3] += static_cast<double>(w * yz);
-                    acc[F_SIGMA + 4] += static_cast<double>(w * xz);
-                    acc[F_SIGMA + 5] += static_cast<double>(w * xy);
-                    if (OBS) {
-                        X *= idr * idr;
-                        float const Xxx = X * xx, Xyy = X * yy, Xzz = X * zz;
-                        acc[F_CB + 0] += static_cast<double>(Xxx * xx);
-                        acc[F_CB + 1] += static_cast<double>(Xyy * yy);
-                        acc[F_CB + 2] += static_cast<double>(Xzz * zz);
-                        acc[F_CB + 3] += static_cast<double>(Xxx * xy);
-                        acc[F_CB + 4] += static_cast<double>(Xxx * xz);
-                        acc[F_CB + 5] += static_cast<double>(Xyy * xy);
-                        acc[F_CB + 6] += static_cast<double>(Xyy * yz);
-                        acc[F_CB + 7] += static_cast<double>(Xzz * xz);
-                        acc[F_CB + 8] += static_cast<double>(Xzz * yz);
-                        acc[F_CB + 9] += static_cast<double>(Xxx * yy);
-                        acc[F_CB + 10] += static_cast<double>(Xxx * zz);
-                        acc[F_CB + 11] += static_cast<double>(Xyy * zz);
-                        acc[F_CB + 12] += static_cast<double>(Xxx * yz);
-                        acc[F_CB + 13] += static_cast<double>(Xyy * xz);
-                        acc[F_CB + 14] += static_cast<double>(Xzz * xy);
-                        acc[F_LAP] += static_cast<double>(lap);
-                    }
-                }
-            }
+            PairSums<OBS> ps;
+            force_row_mx<OBS, true, TPA>(A, T, in, row, nu, sub, fx, fy, fz, epot, ps,
+                                         warn_rmin);
+            force_row_mx<OBS, false, TPA>(A, T, in, row, nd, sub, fx, fy, fz, epot, ps,
+                                          warn_rmin);
             if (warn_rmin)
                 status_or(A.rep + r, MDELAST_WARN_RMIN);
+            s_acc[F_VIRIAL * kBlock + tid] += ps.vir;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                s_acc[(F_SIGMA + k) * kBlock + tid] += ps.sig_d[k];
+                s_acc[(F_SIGMA + 3 + k) * kBlock + tid] += static_cast<double>(ps.sig_o[k]);
+            }
+            if (OBS) {
+#pragma unroll
+                for (int k = 0; k < 15; ++k)
+                    s_acc[(F_CB + k) * kBlock + tid] += static_cast<double>(ps.cb[k]);
+                s_acc[F_LAP * kBlock + tid] += static_cast<double>(ps.lap);
+            }
         }
         fx = group_sum<TPA>(fx);
         fy = group_sum<TPA>(fy);
@@ -353,7 +419,7 @@ __global__ void __launch_bounds__(kBlock) k_force_mx(AtomsView A, TablesView T) 
             A.frc[np + i] = fy;
             A.frc[np + i + np] = fz;
             A.epot[i] = epot;
-            double const m = T.mass[ti];
+            double const m = T.mass[in.ti];
             double vx = A.vel[i], vy = A.vel[np + i], vz = A.vel[2 * np + i];
             if (KICK) {
                 double const e = R->e_kick, cdt = R->cdt_kick;
@@ -364,21 +430,26 @@ __global__ void __launch_bounds__(kBlock) k_force_mx(AtomsView A, TablesView T) 
                 A.vel[np + i] = vy;
                 A.vel[2 * np + i] = vz;
             }
-            acc[F_F2] += fx * fx + fy * fy + fz * fz;
-            acc[F_EKIN] += 0.5 * m * (vx * vx + vy * vy + vz * vz);
-            acc[F_MVV + 0] += m * vx * vx;
-            acc[F_MVV + 1] += m * vy * vy;
-            acc[F_MVV + 2] += m * vz * vz;
-            acc[F_MVV + 3] += m * vy * vz;
-            acc[F_MVV + 4] += m * vx * vz;
-            acc[F_MVV + 5] += m * vx * vy;
-            acc[F_MV + 0] += vx * m;
-            acc[F_MV + 1] += vy * m;
-            acc[F_MV + 2] += vz * m;
-            acc[F_EPOT] += epot;
+            double *acc = s_acc + tid;
+            acc[F_F2 * kBlock] += fx * fx + fy * fy + fz * fz;
+            acc[F_EKIN * kBlock] += 0.5 * m * (vx * vx + vy * vy + vz * vz);
+            acc[(F_MVV + 0) * kBlock] += m * vx * vx;
+            acc[(F_MVV + 1) * kBlock] += m * vy * vy;
+            acc[(F_MVV + 2) * kBlock] += m * vz * vz;
+            acc[(F_MVV + 3) * kBlock] += m * vy * vz;
+            acc[(F_MVV + 4) * kBlock] += m * vx * vz;
+            acc[(F_MVV + 5) * kBlock] += m * vx * vy;
+            acc[(F_MV + 0) * kBlock] += vx * m;
+            acc[(F_MV + 1) * kBlock] += vy * m;
+            acc[(F_MV + 2) * kBlock] += vz * m;
+            acc[F_EPOT * kBlock] += epot;
         }
     }
     // pair sums from eV (and eV/A^2 for the Laplacian) to cgs
+    double acc[F_NSUM];
+#pragma unroll
+    for (int k = 0; k < F_NSUM; ++k)
+        acc[k] = s_acc[k * kBlock + tid];
     acc[F_VIRIAL] *= kEv;
 #pragma unroll
     for (int k = 0; k < 6; ++k)
