@@ -763,6 +763,14 @@ class BatchedMDDriver {
     void set_launch(int td, int tf, int bd, int bf) {
         check(mdelast_driver_set_launch(d_, td, tf, bd, bf));
     }
+    // thermostat (which = 0) or barostat (1) chain of replica r: (q, p_eta, eta)
+    py::tuple chain(int r, int which) {
+        double q[16], p[16], e[16];
+        int32_t n = 0;
+        check(mdelast_batch_get_chain(d_, r, which, q, p, e, &n));
+        return py::make_tuple(std::vector<double>(q, q + n), std::vector<double>(p, p + n),
+                              std::vector<double>(e, e + n));
+    }
     py::dict drain_samples(int r) {
         if (r < 0 || r >= n_replicas())
             throw py::index_error("replica index out of range");
@@ -995,6 +1003,7 @@ PYBIND11_MODULE(md_driver_module, m) {
              py::arg("tpa_force"), py::arg("blocks_density"), py::arg("blocks_force"))
         .def("set_sample_ring", &BatchedMDDriver::set_sample_ring, py::arg("capacity"))
         .def("drain_samples", &BatchedMDDriver::drain_samples, py::arg("replica"))
+        .def("chain", &BatchedMDDriver::chain, py::arg("replica"), py::arg("which") = 0)
         .def("fluctuation_start", &BatchedMDDriver::fluctuation_start)
         .def("fluctuations", &BatchedMDDriver::fluctuations, py::arg("replica"))
         .def("elastic_constants", &BatchedMDDriver::elastic_constants, py::arg("replica"),

@@ -209,13 +209,16 @@ __global__ void __launch_bounds__(kBlock) k_density_mx(AtomsView A, TablesView T
 }
 
 // Sums over the pairs of one lane's share of an atom row, added into the FP64 block
-// accumulators once per row. The virial and the diagonal Born stress are summed in FP64
-// pair by pair (the reference checks the virial against the stress trace to 1e-7,
-// md_driver.cpp:422-429); the off-diagonal stress, Born tensor and Laplacian terms are
+// accumulators once per row. The diagonal Born stress is summed in FP64 pair by pair and
+// the virial is taken as its trace (the sum over pairs of dE/dr r equals that of
+// dE/dr x_a^2 / r): the reference checks the virial against the stress trace to 1e-7 and
+// the pressure against the stress trace to 1e-5 (md_driver.cpp:422-429, 693-698), and near
+// zero pressure, where kinetic and virial parts cancel, that holds only if both come from
+// the same FP32 pair terms. The off-diagonal stress, Born tensor and Laplacian terms are
 // summed in FP32 along the row (at most ~20 FP32 terms, no error beyond the terms' own)
 // and in FP64 across rows and atoms.
 template <bool OBS> struct PairSums {
-    double vir = 0., sig_d[3] = {0., 0., 0.};
+    double sig_d[3] = {0., 0., 0.};
     float sig_o[3] = {0, 0, 0};
     float cb[OBS ? 15 : 1] = {};
     float lap = 0.f;
@@ -314,7 +317,6 @@ __device__ __forceinline__ void force_row_mx(AtomsView const &A, TablesView cons
         fz += static_cast<double>(__fmul_rn(sc, dz));
         epot += static_cast<double>(0.5f * V);
         if (UPPER) {
-            ps.vir += static_cast<double>(dr * dedr);
             float const xx = dx * dx, yy = dy * dy, zz = dz * dz;
             float const yz = dy * dz, xz = dx * dz, xy = dx * dy;
             float const w = dedr * idr;
@@ -389,7 +391,7 @@ __global__ void __launch_bounds__(kBlock) k_force_mx(AtomsView A, TablesView T) 
                                           warn_rmin);
             if (warn_rmin)
                 status_or(A.rep + r, MDELAST_WARN_RMIN);
-            s_acc[F_VIRIAL * kBlock + tid] += ps.vir;
+            s_acc[F_VIRIAL * kBlock + tid] += (ps.sig_d[0] + ps.sig_d[1]) + ps.sig_d[2];
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
                 s_acc[(F_SIGMA + k) * kBlock + tid] += ps.sig_d[k];
