@@ -338,6 +338,33 @@ int mdelast_batch_get_fluct(mdelast_driver *d, int32_t replica, mdelast_fluct *o
 int mdelast_elastic_constants(const mdelast_fluct *f, int32_t ensemble, double T_thermostat,
                               double P_barostat, double *C, double *summary);
 
+/* ---- Learned warm start: a small MLP trained and evaluated on the device ----
+ * No counterpart in the reference (its runs start from a guessed lattice constant and
+ * equilibrate by NPT). Fully connected layers of the given widths, GELU between layers,
+ * linear output, FP32; loss = mean squared error over all outputs; Adam (lr, beta 0.9 /
+ * 0.999, eps 1e-8), full batch. Parameters: per layer W (in x out, row-major) then b (out).
+ * Training is deterministic (fixed-order sums, no atomics). */
+typedef struct mdelast_mlp_s mdelast_mlp;
+#define MDELAST_MLP_MAX_LAYERS 8
+/* widths: n_layers + 1 values (inputs, hidden widths, outputs). Glorot-normal weights and
+ * zero biases drawn from `seed`. */
+int mdelast_mlp_create(int32_t n_layers, const int32_t *widths, uint64_t seed, int32_t device,
+                       mdelast_mlp **out);
+void mdelast_mlp_destroy(mdelast_mlp *m);
+int mdelast_mlp_n_params(const mdelast_mlp *m, int64_t *n);
+int mdelast_mlp_get_params(mdelast_mlp *m, float *out);
+/* also resets the optimiser state */
+int mdelast_mlp_set_params(mdelast_mlp *m, const float *in);
+/* y (n x outputs) = f(x (n x inputs)); host arrays */
+int mdelast_mlp_forward(mdelast_mlp *m, const float *x, int32_t n, float *y);
+/* loss and its gradient with respect to every parameter (host arrays; either output may
+ * be NULL), without changing the parameters */
+int mdelast_mlp_gradients(mdelast_mlp *m, const float *x, const float *y, int32_t n,
+                          float *loss, float *grad);
+/* `steps` Adam steps on (x, y); *loss (may be NULL) = the loss after the last step */
+int mdelast_mlp_train(mdelast_mlp *m, const float *x, const float *y, int32_t n,
+                      int32_t steps, float lr, float *loss);
+
 /* g(r) that allocates nothing. No counterpart in the reference: it exists for callers
  * that may not allocate device memory when they sample g(r), for example an application
  * whose allocator owns all device memory and forbids third-party cudaMalloc/cudaFree, or

@@ -23,7 +23,7 @@ INCLUDE = os.path.join(ROOT, "include")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CUDA_SOURCES = ["atom_kernels.cu", "mixed_kernels.cu", "scalar_kernels.cu", "gr_kernels.cu", "gr_static.cu", "driver.cu"]
+CUDA_SOURCES = ["atom_kernels.cu", "mixed_kernels.cu", "scalar_kernels.cu", "gr_kernels.cu", "gr_static.cu", "mlp.cu", "driver.cu"]
 HOST_SOURCES = ["host_tables.cpp", "host_fluct.cpp"]
 
 

@@ -178,3 +178,54 @@ def time_to_within(result: ProtocolResult, target: dict, tol: float = 0.02):
         elif not good:
             ok_from = None
     return ok_from
+
+
+def run_warm_start(m, tables, cells: list[Cell], precision="mixed",
+                   stages: Stages | None = None, judge=None, check_steps=1000,
+                   fallback: Stages | None = None, autotune=True) -> ProtocolResult:
+    """The production run started in a proposed equilibrium box (`cells`, NVT, built at
+    the proposed lattice constant), with no NPT stage: NVT thermalisation, then production
+    whose first `check_steps` steps also serve as the acceptance window. If `judge(p_GPa)`
+    rejects any replica's mean pressure over that window, the proposal is discarded and
+    the plain protocol (run_protocol with `fallback` stages) runs from the same cells."""
+    st = stages or Stages(npt_therm=0, npt_prod=0, nvt_therm=1000, nvt_prod=2000,
+                          sample_stride=5, checkpoint_every=500)
+    t0 = time.perf_counter()
+    b = make_batch(m, tables, [replace(c, ensemble=1) for c in cells], r_skin=1.2,
+                   precision=precision)
+    if autotune:
+        b.autotune(2)
+    b.run(st.nvt_therm, st.rebuild_every, st.sample_stride, False)
+    for r in range(b.n_replicas):
+        b.drain_samples(r)
+    b.fluctuation_start()
+    n = min(check_steps, st.nvt_prod)
+    b.run(n, st.rebuild_every, st.sample_stride, False)
+    p = [float(np.mean(b.drain_samples(r)["pressure"])) / U.GPa for r in range(b.n_replicas)]
+    if judge is not None and not all(judge(x) for x in p):
+        del b
+        res = run_protocol(m, tables, cells, precision=precision, stages=fallback or Stages(),
+                           autotune=autotune)
+        res.accepted_start = False
+        res.wall_s = time.perf_counter() - t0
+        return res
+    b.set_sample_ring(0)
+    done, checkpoints, Cr = n, [], []
+    while True:
+        if done % st.checkpoint_every == 0 or done >= st.nvt_prod:
+            Cr = [b.elastic_constants(r) for r in range(b.n_replicas)]
+            C = [float(np.mean([c[k] for c in Cr])) / U.GPa for k in ("C11", "C12", "C44")]
+            checkpoints.append((done, time.perf_counter() - t0, *C))
+        if done >= st.nvt_prod:
+            break
+        k = min(st.checkpoint_every - done % st.checkpoint_every, st.nvt_prod - done)
+        b.run(k, st.rebuild_every, st.sample_stride, False)
+        done += k
+    wall = time.perf_counter() - t0
+    C_rep = [{k: c[k] / U.GPa for k in ("C11", "C12", "C44")} for c in Cr]
+    C = {k: float(np.mean([c[k] for c in C_rep])) for k in ("C11", "C12", "C44")}
+    return ProtocolResult(precision=precision, replicas=len(cells),
+                          atoms_per_replica=cells[0].n_atoms, stages=st,
+                          V_V0=[1.0] * len(cells), npt_pressure_GPa=p, C=C, C_replicas=C_rep,
+                          checkpoints=checkpoints, wall_s=wall, wall_npt_s=0.0,
+                          accepted_start=True)
