@@ -16,6 +16,10 @@ plain path (one FP64 cell, L2 flushed before every timed step) is reported besid
 e2e = the same batched metric through the public API: the batch created from host arrays,
 every step the per-replica observables molecular_dynamics.py's append_sample reads, the
 final positions and velocities read back; wall-clock time of all of it.
+time_to_cij (rank 0, --no-cij skips it): wall time to C11/C12/C44 within 2 % of the FP64
+plain protocol's result, the plain protocol (one FP64 cell, NPT then NVT as the reference's
+sample case, 120k steps) against 4 mixed-precision replicas started in the box the trained
+warm-start network proposes (see time_to_cij).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--replicas R] [--precision fp64|mixed]
@@ -213,6 +217,9 @@ def run_ours(args, rank, world, local_rank):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_sample(N)
+    cij = None
+    if rank == 0 and not args.no_cij:
+        cij = time_to_cij(m, t, cpu)
     n_rebuilds = (args.steps + REBUILD - 1) // REBUILD
     launches = args.steps * 6 + n_rebuilds * 3
     line = {
@@ -231,6 +238,7 @@ def run_ours(args, rank, world, local_rank):
                    "parallelism": f"replicas only, dp{world}", "fatal_status_clear": status_ok,
                    "launch": tune},
         "plain_fp64_single_cell": plain,
+        "time_to_cij": cij,
         "roofline": roof,
         "cpu_baseline": cpu,
         "e2e": None if args.no_e2e else {
@@ -259,6 +267,77 @@ def make_cells(replicas, seed0=0):
     cells = [cuzn_cell(t, NSIDE, n_zn=N_ZN, T=T_K, ensemble=1, placement_seed=42,
                        velocity_seed=seed0 + k) for k in range(replicas)]
     return t, cells
+
+
+# ----------------------------------------------------------------------------- time to C_ij
+CIJ_TOL = 0.02
+PLAIN_STAGES = dict(npt_therm=10000, npt_prod=10000, nvt_therm=10000, nvt_prod=90000,
+                    sample_stride=1, rebuild_every=REBUILD, checkpoint_every=2500)
+WARM_REPLICAS = 4
+WARM_STAGES = dict(npt_therm=0, npt_prod=0, nvt_therm=500, nvt_prod=3000, sample_stride=5,
+                   rebuild_every=REBUILD, checkpoint_every=250)
+
+
+def time_to_cij(m, t, cpu):
+    """Wall time to C11/C12/C44 of the workload cell at 300 K.
+
+    plain: the reference's protocol in FP64 on the GPU, one cell: 20k NPT steps (10k
+    thermalisation + 10k production for the mean box), handoff into the mean box, 100k NVT
+    steps (10k + 90k production, sampled every step); its final C_ij is the target.
+    warm start: the trained network proposes the zero-pressure lattice constant; 4 replicas
+    of the cell in that box, mixed precision, no NPT stage, 500 NVT thermalisation steps,
+    production sampled every 5th step with the running estimate read every 250 steps;
+    accepted because the first 500 production steps' mean pressure passes the judge (else
+    it would fall back to NPT). Its time counts from loading the network (driver creation,
+    autotuning and every readout included) to the first checkpoint from which all three
+    constants stay within 2 % of the plain result until the end of its run."""
+    from mdelast_b200.protocol import Stages, run_protocol, run_warm_start, time_to_within
+    from mdelast_b200.systems import cuzn_cell
+    from mdelast_b200.warmstart import WarmStart, judge
+    base = dict(n_zn=N_ZN, T=T_K, placement_seed=42)
+    plain = run_protocol(m, t, [cuzn_cell(t, NSIDE, ensemble=2, velocity_seed=0, **base)],
+                         precision="fp64", stages=Stages(**PLAIN_STAGES), nvt_seeds=[1])
+    target = plain.C
+    t0 = time.perf_counter()
+    ws = WarmStart.load()
+    prop = ws.propose(N_ZN / NSIDE**3 / 4, T_K)
+    a = float(prop["a"][0])
+    cells = [cuzn_cell(t, NSIDE, a_ang=a, ensemble=1, velocity_seed=200 + k, **base)
+             for k in range(WARM_REPLICAS)]
+    setup = time.perf_counter() - t0
+    warm = run_warm_start(m, t, cells, precision="mixed", stages=Stages(**WARM_STAGES),
+                          judge=judge, check_steps=500)
+    t_warm = time_to_within(warm, target, CIJ_TOL)
+    t_warm = None if t_warm is None else setup + t_warm
+    t_plain_self = time_to_within(plain, target, CIJ_TOL)
+    out = {
+        "metric": f"wall time to C11/C12/C44 within {CIJ_TOL:.0%} of the FP64 plain result",
+        "unit": "s", "cell": WORKLOAD, "tolerance": CIJ_TOL,
+        "plain_fp64": {"wall_s": plain.wall_s, "C_GPa": plain.C, "steps": 120000,
+                       "replicas": 1, "stages": PLAIN_STAGES,
+                       "own_time_to_within_s": t_plain_self,
+                       "npt_mean_box_V_V0": plain.V_V0[0]},
+        "warm_start_mixed": {"time_to_within_s": t_warm, "wall_s": setup + warm.wall_s,
+                             "C_GPa": warm.C,
+                             "rel_err_vs_plain": {k: warm.C[k] / target[k] - 1 for k in target},
+                             "replicas": WARM_REPLICAS, "stages": WARM_STAGES,
+                             "proposal": {k: float(v[0]) for k, v in prop.items()},
+                             "accepted": warm.accepted_start,
+                             "window_pressure_GPa": warm.npt_pressure_GPa},
+        "speedup_vs_plain_protocol": (plain.wall_s / t_warm) if t_warm else None,
+        "speedup_vs_plain_time_to_within": (t_plain_self / t_warm)
+        if (t_warm and t_plain_self) else None,
+    }
+    if cpu and cpu.get("value"):
+        # the reference core's measured per-step time on this host, times the plain protocol
+        ms_step = 1e3 * NSIDE**3 * 4 / cpu["value"]
+        est = 120000 * ms_step * 1e-3
+        out["reference_cpu_estimated_s"] = est
+        out["reference_cpu_basis"] = (f"{ms_step:.1f} ms/step measured for the reference core "
+                                      f"(1 core, cpu_baseline) x 120,000 steps; not run")
+        if t_warm:
+            out["speedup_vs_reference_cpu_estimated"] = est / t_warm
+    return out
 
 
 def half_list_nbar(m, t, cell):
@@ -362,6 +441,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cij", action="store_true",
+                    help="skip the time-to-C_ij comparison (plain FP64 protocol vs warm start)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
