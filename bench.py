@@ -193,19 +193,26 @@ def run_ours(args, rank, world, local_rank):
     e2e_steps = max(args.steps, REBUILD)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
+    phases = {}
     if not args.no_e2e:
         bb = make_batch(m, t, cells, dt=DT, r_skin=SKIN, precision=args.precision,
                         device=local_rank)
         # the shapes tuned above for this workload, reused as a caller would
         bb.set_launch(tune["tpa_density"], tune["tpa_force"], tune["blocks_density"],
                       tune["blocks_force"])
+        t1 = time.perf_counter()
         for s in range(e2e_steps):
             bb.run(1, REBUILD, 1, False)
             for r in range(bb.n_replicas):
                 _ = bb.observables(r)
+        t2 = time.perf_counter()
         for r in range(bb.n_replicas):
             _ = (bb.atoms(r, m.ATOM_POSITIONS), bb.atoms(r, m.ATOM_VELOCITIES))
+        t3 = time.perf_counter()
         del bb
+        t4 = time.perf_counter()
+        phases = {"create_s": t1 - t0, "steps_s": t2 - t1, "readback_s": t3 - t2,
+                  "destroy_s": t4 - t3}
     t_e2e = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device="cuda")
     if dist is not None:
         dist.all_reduce(t_e2e, op=dist.ReduceOp.MAX)
@@ -220,6 +227,7 @@ def run_ours(args, rank, world, local_rank):
     cij = None
     if rank == 0 and not args.no_cij:
         cij = time_to_cij(m, t, cpu)
+    others = None if args.no_configs else other_configs(m, t, local_rank)
     n_rebuilds = (args.steps + REBUILD - 1) // REBUILD
     launches = args.steps * 6 + n_rebuilds * 3
     line = {
@@ -239,12 +247,14 @@ def run_ours(args, rank, world, local_rank):
                    "launch": tune},
         "plain_fp64_single_cell": plain,
         "time_to_cij": cij,
+        "other_configs": others,
         "roofline": roof,
         "cpu_baseline": cpu,
         "e2e": None if args.no_e2e else {
             "value": e2e_value, "unit": "atom-steps/s",
             "h2d_bytes_per_step": h2d / e2e_steps, "d2h_bytes_per_step": d2h / e2e_steps,
-            "steps": e2e_steps, "api": "md_driver_module.BatchedMDDriver"},
+            "steps": e2e_steps, "api": "md_driver_module.BatchedMDDriver",
+            "phases": phases},
         "gpu_launches": launches,
         "clocks": clocks,
     }
@@ -253,6 +263,26 @@ def run_ours(args, rank, world, local_rank):
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def other_configs(m, t, device, steps=50, warmup=5):
+    """Atom-steps/s of the other batched and single-cell workloads, mixed precision,
+    observables every step, list rebuilt every 20 steps, autotuned, CUDA-event timed:
+    64 uneven replicas (4 n^3 atoms, n uniform in [4, 20], x_Zn in [0, 0.3], T in [5, 900] K,
+    from RandomState(2026)) and the 32,000-atom L1_2 CuZn3 cell at 5 K."""
+    from mdelast_b200.systems import l12_cell, make_batch, uneven_replicas
+    out = {}
+    for name, cells in [("batched_uneven_64", uneven_replicas(t, 64)),
+                        ("l12_cuzn3_20x20x20_5K", [l12_cell(t, 20, T=5.0, ensemble=1)])]:
+        b = make_batch(m, t, cells, dt=DT, r_skin=SKIN, precision="mixed", device=device)
+        tune = b.autotune(2)
+        b.run(warmup, REBUILD, 1, False)
+        ms = b.run(steps, REBUILD, 1, True)
+        out[name] = {"value": b.n_atoms * steps / (ms * 1e-3), "unit": "atom-steps/s",
+                     "atoms": b.n_atoms, "replicas": b.n_replicas, "steps": steps,
+                     "ms_per_step": ms / steps, "launch": tune}
+        del b
+    return out
 
 
 def make_cells(replicas, seed0=0):
@@ -351,7 +381,7 @@ def half_list_nbar(m, t, cell):
 # ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_force_mx launch
 # (profiles/k_force_mx_k_density_mx_bench_4x13500.md, 4 replicas, cold caches); the
 # 16- and 32-replica entries scale it by the atoms processed. None where not captured.
-_TRAFFIC_4 = 53.228288e6 + 0.228352e6
+_TRAFFIC_4 = 53.211904e6 + 0.262656e6
 TRAFFIC_PER_LAUNCH: dict = {("mixed", 4): _TRAFFIC_4, ("mixed", 16): 4 * _TRAFFIC_4,
                             ("mixed", 32): 8 * _TRAFFIC_4}
 
@@ -441,6 +471,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other workloads (64 uneven replicas, L1_2 32k cell)")
     ap.add_argument("--no-cij", action="store_true",
                     help="skip the time-to-C_ij comparison (plain FP64 protocol vs warm start)")
     args = ap.parse_args()

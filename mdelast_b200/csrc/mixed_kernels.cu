@@ -93,13 +93,28 @@ __global__ void k_posf(AtomsView A) {
                             static_cast<float>(c.w));
 }
 
+// Sum v over the warp (fixed order) and add it to this warp's shared accumulator.
+__device__ __forceinline__ void warp_accumulate(double v, double *slot) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0)
+        *slot += v;
+}
+
 // Density pass of md_driver.cpp:195-277 in mixed precision (see k_density for the roles).
+// The block's FP64 sums (embedding energy, the per-atom Born term F''_i g_i g_i^T and
+// Laplacian term) are folded warp by warp after each atom group into per-warp shared
+// accumulators instead of being carried in registers through the pair loop: the loop then
+// runs with about half the registers, so twice the warps per SM hide the latency of the
+// partner gathers.
 template <bool OBS, int TPA>
 __global__ void __launch_bounds__(kBlock) k_density_mx(AtomsView A, TablesView T) {
-    double acc[D_NSUM];
-#pragma unroll
-    for (int k = 0; k < D_NSUM; ++k)
-        acc[k] = 0.;
+    __shared__ double sacc[kBlock / 32][D_NSUM];
+    int const warp = threadIdx.x >> 5;
+    for (int k = threadIdx.x; k < (kBlock / 32) * D_NSUM; k += kBlock)
+        (&sacc[0][0])[k] = 0.;
+    __syncthreads();
     int const r = A.dblk_rep[blockIdx.x];
     Replica const *R = A.rep + r;
     int const lb = blockIdx.x - R->dblk_begin, nb = R->dblk_n;
@@ -107,6 +122,7 @@ __global__ void __launch_bounds__(kBlock) k_density_mx(AtomsView A, TablesView T
     int const n_slots = R->n_blocks * kBlock;
     float3 L, iL;
     box_f(R, L, iL);
+    double const a3 = kAng * kAng * kAng;
     for (int a0 = lb * apb; a0 < n_slots; a0 += nb * apb) {
         int const a = a0 + static_cast<int>(threadIdx.x) / TPA;
         int const i = R->atom_begin + a;
@@ -128,7 +144,8 @@ __global__ void __launch_bounds__(kBlock) k_density_mx(AtomsView A, TablesView T
                 float const r2 = min_image_f(pi, pj, L, iL, dx, dy, dz);
                 if (r2 > T.fr_cut_sq)
                     continue;
-                float const dr = sqrtf(r2);
+                float const idr = rsqrtf(r2);
+                float const dr = __fmul_rn(r2, idr);
                 int const tj = static_cast<int>(pj.w);
                 if (dr > T.feam_rcut[tj])
                     continue;
@@ -139,7 +156,7 @@ __global__ void __launch_bounds__(kBlock) k_density_mx(AtomsView A, TablesView T
                 ld6f(T.rbf + (static_cast<size_t>(pair_slot(ti, tj)) * T.nri + k) * 18 + off, c);
                 rho += tabf_v(c, t);
                 if (OBS) {
-                    float const ar = tabf_d1(c, t, T.finv_hr) / dr;
+                    float const ar = tabf_d1(c, t, T.finv_hr) * idr;
                     float const ap[3] = {ar * dx, ar * dy, ar * dz};
                     g[0] += ap[0] * dx;
                     g[1] += ap[1] * dy;
@@ -162,21 +179,23 @@ __global__ void __launch_bounds__(kBlock) k_density_mx(AtomsView A, TablesView T
             for (int u = 0; u < 3; ++u)
                 hv[u] = group_sum<TPA>(hv[u]);
         }
-        if (valid && sub == 0) {
+        double F = 0., d2F = 0.;
+        bool const own = valid && sub == 0;
+        if (own) {
             // the embedding function in FP64 and cgs (eam.hpp:48-70)
-            double const rc = static_cast<double>(rho) / (kAng * kAng * kAng);
+            double const rc = static_cast<double>(rho) / a3;
             if (rc > T.rhomax[ti])
                 status_or(A.rep + r, MDELAST_FATAL_RHO_MAX);
             double t;
             int const k = tab_locate(rc, T.inv_hf, T.nfi, t);
             double c[6];
             ld6(T.Ft + (static_cast<size_t>(ti) * T.nfi + k) * 6, c);
-            double const F = tab_v(c, t), dF = tab_d1(c, t, T.inv_hf);
-            double const d2F = OBS ? tab_d2(c, t, T.inv_hf2) : 0.;
+            F = tab_v(c, t);
+            double const dF = tab_d1(c, t, T.inv_hf);
+            d2F = OBS ? tab_d2(c, t, T.inv_hf2) : 0.;
             A.rho[i] = rc;
             A.Fe[i] = F;
             // F' [erg cm^3] -> [eV A^3] and F'' [erg cm^6] -> [eV A^6]
-            double const a3 = kAng * kAng * kAng;
             if (OBS) {
                 A.dF2[i] = make_double2(dF, d2F);
                 A.dF2f[i] = make_float2(static_cast<float>(dF / (a3 * kEv)),
@@ -185,27 +204,33 @@ __global__ void __launch_bounds__(kBlock) k_density_mx(AtomsView A, TablesView T
                 A.dF2[i].x = dF;
                 A.dF2f[i].x = static_cast<float>(dF / (a3 * kEv));
             }
-            acc[D_FSUM] += F;
-            if (OBS) {
-                // g in cm^-3 and h in cm^-4, as the cgs F'' expects
-                double gc[6], hc[3];
+        }
+        warp_accumulate(F, &sacc[warp][D_FSUM]);
+        if (OBS) {
+            // g in cm^-3 and h in cm^-4, as the cgs F'' expects; zero for lanes without an atom
+            double gc[6];
 #pragma unroll
-                for (int u = 0; u < 6; ++u)
-                    gc[u] = static_cast<double>(g[u]) / a3;
+            for (int u = 0; u < 6; ++u)
+                gc[u] = own ? static_cast<double>(g[u]) / a3 : 0.;
+            int q = D_CB;
 #pragma unroll
-                for (int u = 0; u < 3; ++u)
-                    hc[u] = static_cast<double>(hv[u]) / (a3 * kAng);
-                int q = D_CB;
+            for (int u = 0; u < 6; ++u)
 #pragma unroll
-                for (int u = 0; u < 6; ++u)
-#pragma unroll
-                    for (int v = u; v < 6; ++v)
-                        acc[q++] += d2F * gc[u] * gc[v];
-                acc[D_LAP] += d2F * (hc[0] * hc[0] + hc[1] * hc[1] + hc[2] * hc[2]);
-            }
+                for (int v = u; v < 6; ++v)
+                    warp_accumulate(d2F * gc[u] * gc[v], &sacc[warp][q++]);
+            double const ha = a3 * kAng;
+            double const h0 = hv[0] / ha, h1 = hv[1] / ha, h2 = hv[2] / ha;
+            warp_accumulate(own ? d2F * (h0 * h0 + h1 * h1 + h2 * h2) : 0., &sacc[warp][D_LAP]);
         }
     }
-    block_sum_store<D_NSUM>(acc, A.pd + static_cast<size_t>(blockIdx.x) * D_NSUM);
+    __syncthreads();
+    for (int k = threadIdx.x; k < D_NSUM; k += blockDim.x) {
+        double s = 0.;
+#pragma unroll
+        for (int w = 0; w < kBlock / 32; ++w)
+            s += sacc[w][k];
+        A.pd[static_cast<size_t>(blockIdx.x) * D_NSUM + k] = s;
+    }
 }
 
 // Sums over the pairs of one lane's share of an atom row, added into the FP64 block
