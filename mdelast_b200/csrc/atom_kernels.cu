@@ -168,8 +168,9 @@ __global__ void k_nbr_build(AtomsView A) {
 // so those per-atom Born and Laplacian terms (md_driver.cpp:410-419) are formed here and
 // g, h are never stored.
 
-template <bool OBS, int TPA>
+template <bool OBS, int TPA, int IP>
 __global__ void __launch_bounds__(kBlock) k_density(AtomsView A, TablesView T) {
+    constexpr int kF = TabFmt<IP>::kF;
     int const r = A.dblk_rep[blockIdx.x];
     Replica const *R = A.rep + r;
     int const lb = blockIdx.x - R->dblk_begin, nb = R->dblk_n;
@@ -209,12 +210,14 @@ __global__ void __launch_bounds__(kBlock) k_density(AtomsView A, TablesView T) {
             double t;
             int const k = tab_locate(dr, T.inv_hr, T.nri, t);
             int const s = pair_slot(ti, tj);
-            int const off = (tj == (ti < tj ? ti : tj)) ? 6 : 12;
-            double c[6];
-            ld6(T.rb + (static_cast<size_t>(s) * T.nri + k) * 18 + off, c);
-            rho += tab_v(c, t);
+            int const off = (tj == (ti < tj ? ti : tj)) ? kF : 2 * kF;
+            double v = 0., d1 = 0., d2 = 0.;
+            tab_eval<IP, true, OBS, false>(T.rb + (static_cast<size_t>(s) * T.nri + k) * 3 * kF +
+                                               off,
+                                           t, T.inv_hr, T.inv_hr2, v, d1, d2);
+            rho += v;
             if (OBS) {
-                double const ar = tab_d1(c, t, T.inv_hr) / dr;
+                double const ar = d1 / dr;
                 double const ap[3] = {ar * px, ar * py, ar * pz};
                 g[0] += ap[0] * px;
                 g[1] += ap[1] * py;
@@ -244,10 +247,9 @@ __global__ void __launch_bounds__(kBlock) k_density(AtomsView A, TablesView T) {
             status_or(A.rep + r, MDELAST_FATAL_RHO_MAX);
         double t;
         int const k = tab_locate(rho, T.inv_hf, T.nfi, t);
-        double c[6];
-        ld6(T.Ft + (static_cast<size_t>(ti) * T.nfi + k) * 6, c);
-        double const F = tab_v(c, t), dF = tab_d1(c, t, T.inv_hf);
-        double const d2F = OBS ? tab_d2(c, t, T.inv_hf2) : 0.;
+        double F = 0., dF = 0., d2F = 0.;
+        tab_eval<IP, true, true, OBS>(T.Ft + (static_cast<size_t>(ti) * T.nfi + k) * kF, t,
+                                      T.inv_hf, T.inv_hf2, F, dF, d2F);
         A.rho[i] = rho;
         A.Fe[i] = F;
         if (OBS)
@@ -277,8 +279,9 @@ __global__ void __launch_bounds__(kBlock) k_density(AtomsView A, TablesView T) {
 // its j > i visit; the Born tensor is accumulated as the 15 distinct degree-4 monomials
 // X p_a p_b p_c p_d of which its 21 upper-triangle entries are made.
 
-template <bool OBS, bool KICK, int TPA>
+template <bool OBS, bool KICK, int TPA, int IP>
 __global__ void __launch_bounds__(kBlock) k_force(AtomsView A, TablesView T) {
+    constexpr int kF = TabFmt<IP>::kF;
     int const r = A.fblk_rep[blockIdx.x];
     Replica const *R = A.rep + r;
     int const lb = blockIdx.x - R->fblk_begin, nb = R->fblk_n;
@@ -326,19 +329,13 @@ __global__ void __launch_bounds__(kBlock) k_force(AtomsView A, TablesView T) {
             int const s = pair_slot(ti, tj);
             double t;
             int const k = tab_locate(dr, T.inv_hr, T.nri, t);
-            const double *bundle = T.rb + (static_cast<size_t>(s) * T.nri + k) * 18;
+            const double *bundle = T.rb + (static_cast<size_t>(s) * T.nri + k) * 3 * kF;
             // TablePotential::calculate (potential.hpp:92-104)
             double V = 0., dV = 0., d2V = 0.;
             if (dr < T.pot_rmin[s])
                 warn_rmin = true;
-            if (!(dr > T.pot_rcut[s])) {
-                double c[6];
-                ld6(bundle, c);
-                V = tab_v(c, t);
-                dV = tab_d1(c, t, T.inv_hr);
-                if (OBS)
-                    d2V = tab_d2(c, t, T.inv_hr2);
-            }
+            if (!(dr > T.pot_rcut[s]))
+                tab_eval<IP, true, true, OBS>(bundle, t, T.inv_hr, T.inv_hr2, V, dV, d2V);
             double dedr = dV;
             double X = 0., lap = 0.;
             if (OBS) {
@@ -346,23 +343,15 @@ __global__ void __launch_bounds__(kBlock) k_force(AtomsView A, TablesView T) {
                 lap = 2. * (d2V + 2. * dV * idr);
             }
             if (T.has_eam) {
-                // rho of the lower type at bundle offset 6, of the higher type at 12
-                int const oi = (ti <= tj) ? 6 : 12, oj = (ti < tj) ? 12 : 6;
-                double drho_i = 0., drho_j = 0., d2rho_i = 0., d2rho_j = 0.;
-                if (!(dr > T.eam_rcut[ti])) {
-                    double c[6];
-                    ld6(bundle + oi, c);
-                    drho_i = tab_d1(c, t, T.inv_hr);
-                    if (OBS)
-                        d2rho_i = tab_d2(c, t, T.inv_hr2);
-                }
-                if (!(dr > T.eam_rcut[tj])) {
-                    double c[6];
-                    ld6(bundle + oj, c);
-                    drho_j = tab_d1(c, t, T.inv_hr);
-                    if (OBS)
-                        d2rho_j = tab_d2(c, t, T.inv_hr2);
-                }
+                // rho of the lower type at bundle offset kF, of the higher type at 2 kF
+                int const oi = (ti <= tj) ? kF : 2 * kF, oj = (ti < tj) ? 2 * kF : kF;
+                double drho_i = 0., drho_j = 0., d2rho_i = 0., d2rho_j = 0., unused = 0.;
+                if (!(dr > T.eam_rcut[ti]))
+                    tab_eval<IP, false, true, OBS>(bundle + oi, t, T.inv_hr, T.inv_hr2, unused,
+                                                   drho_i, d2rho_i);
+                if (!(dr > T.eam_rcut[tj]))
+                    tab_eval<IP, false, true, OBS>(bundle + oj, t, T.inv_hr, T.inv_hr2, unused,
+                                                   drho_j, d2rho_j);
                 double const dFj = dFj2.x;
                 // the two cross terms are rounded separately and added (commutative), so
                 // the i- and j-side evaluations of dE/dr are bitwise equal
@@ -602,14 +591,19 @@ __global__ void k_table_eval(TablesView T, int which, int s, const double *x, in
     if (q >= n)
         return;
     double const xv = x[q];
-    double t, c[6];
+    double t;
     double v[3] = {0., 0., 0.};
+    bool const bs = T.interp == MDELAST_BSPLINE;
+    int const kF = bs ? TabFmt<MDELAST_BSPLINE>::kF : TabFmt<MDELAST_QUINTIC>::kF;
     if (which == 2) {
         int const k = tab_locate(xv, T.inv_hf, T.nfi, t);
-        ld6(T.Ft + (static_cast<size_t>(s) * T.nfi + k) * 6, c);
-        v[0] = tab_v(c, t);
-        v[1] = tab_d1(c, t, T.inv_hf);
-        v[2] = tab_d2(c, t, T.inv_hf2);
+        const double *p = T.Ft + (static_cast<size_t>(s) * T.nfi + k) * kF;
+        if (bs)
+            tab_eval<MDELAST_BSPLINE, true, true, true>(p, t, T.inv_hf, T.inv_hf2, v[0], v[1],
+                                                        v[2]);
+        else
+            tab_eval<MDELAST_QUINTIC, true, true, true>(p, t, T.inv_hf, T.inv_hf2, v[0], v[1],
+                                                        v[2]);
     } else {
         int const k = tab_locate(xv, T.inv_hr, T.nri, t);
         int slot, off;
@@ -620,14 +614,17 @@ __global__ void k_table_eval(TablesView T, int which, int s, const double *x, in
             rc = T.pot_rcut[s];
         } else {
             slot = pair_slot(s, s);
-            off = 6;
+            off = kF;
             rc = T.eam_rcut[s];
         }
         if (!(xv > rc)) {
-            ld6(T.rb + (static_cast<size_t>(slot) * T.nri + k) * 18 + off, c);
-            v[0] = tab_v(c, t);
-            v[1] = tab_d1(c, t, T.inv_hr);
-            v[2] = tab_d2(c, t, T.inv_hr2);
+            const double *p = T.rb + (static_cast<size_t>(slot) * T.nri + k) * 3 * kF + off;
+            if (bs)
+                tab_eval<MDELAST_BSPLINE, true, true, true>(p, t, T.inv_hr, T.inv_hr2, v[0],
+                                                            v[1], v[2]);
+            else
+                tab_eval<MDELAST_QUINTIC, true, true, true>(p, t, T.inv_hr, T.inv_hr2, v[0],
+                                                            v[1], v[2]);
         }
     }
     out[3 * q] = v[0];
@@ -636,23 +633,43 @@ __global__ void k_table_eval(TablesView T, int which, int s, const double *x, in
 }
 
 namespace {
-template <bool OBS> void density_tpa(int tpa, int grid, cudaStream_t s, AtomsView const &A,
-                                     TablesView const &T) {
+template <bool OBS, int IP>
+void density_tpa(int tpa, int grid, cudaStream_t s, AtomsView const &A, TablesView const &T) {
     switch (tpa) {
-    case 1: k_density<OBS, 1><<<grid, kBlock, 0, s>>>(A, T); break;
-    case 4: k_density<OBS, 4><<<grid, kBlock, 0, s>>>(A, T); break;
-    case 8: k_density<OBS, 8><<<grid, kBlock, 0, s>>>(A, T); break;
-    default: k_density<OBS, 16><<<grid, kBlock, 0, s>>>(A, T); break;
+    case 1: k_density<OBS, 1, IP><<<grid, kBlock, 0, s>>>(A, T); break;
+    case 4: k_density<OBS, 4, IP><<<grid, kBlock, 0, s>>>(A, T); break;
+    case 8: k_density<OBS, 8, IP><<<grid, kBlock, 0, s>>>(A, T); break;
+    default: k_density<OBS, 16, IP><<<grid, kBlock, 0, s>>>(A, T); break;
     }
 }
-template <bool OBS, bool KICK>
+template <bool OBS, bool KICK, int IP>
 void force_tpa(int tpa, int grid, cudaStream_t s, AtomsView const &A, TablesView const &T) {
     switch (tpa) {
-    case 1: k_force<OBS, KICK, 1><<<grid, kBlock, 0, s>>>(A, T); break;
-    case 4: k_force<OBS, KICK, 4><<<grid, kBlock, 0, s>>>(A, T); break;
-    case 8: k_force<OBS, KICK, 8><<<grid, kBlock, 0, s>>>(A, T); break;
-    default: k_force<OBS, KICK, 16><<<grid, kBlock, 0, s>>>(A, T); break;
+    case 1: k_force<OBS, KICK, 1, IP><<<grid, kBlock, 0, s>>>(A, T); break;
+    case 4: k_force<OBS, KICK, 4, IP><<<grid, kBlock, 0, s>>>(A, T); break;
+    case 8: k_force<OBS, KICK, 8, IP><<<grid, kBlock, 0, s>>>(A, T); break;
+    default: k_force<OBS, KICK, 16, IP><<<grid, kBlock, 0, s>>>(A, T); break;
     }
+}
+template <int IP>
+void density_ip(bool obs, int tpa, int grid, cudaStream_t s, AtomsView const &A,
+                TablesView const &T) {
+    if (obs)
+        density_tpa<true, IP>(tpa, grid, s, A, T);
+    else
+        density_tpa<false, IP>(tpa, grid, s, A, T);
+}
+template <int IP>
+void force_ip(bool obs, bool kick, int tpa, int grid, cudaStream_t s, AtomsView const &A,
+              TablesView const &T) {
+    if (obs && kick)
+        force_tpa<true, true, IP>(tpa, grid, s, A, T);
+    else if (obs)
+        force_tpa<true, false, IP>(tpa, grid, s, A, T);
+    else if (kick)
+        force_tpa<false, true, IP>(tpa, grid, s, A, T);
+    else
+        force_tpa<false, false, IP>(tpa, grid, s, A, T);
 }
 } // namespace
 
@@ -660,22 +677,18 @@ bool valid_tpa(int tpa) { return tpa == 1 || tpa == 4 || tpa == 8 || tpa == 16; 
 
 void launch_density(bool obs, int tpa, int grid, cudaStream_t s, AtomsView const &A,
                     TablesView const &T) {
-    if (obs)
-        density_tpa<true>(tpa, grid, s, A, T);
+    if (T.interp == MDELAST_BSPLINE)
+        density_ip<MDELAST_BSPLINE>(obs, tpa, grid, s, A, T);
     else
-        density_tpa<false>(tpa, grid, s, A, T);
+        density_ip<MDELAST_QUINTIC>(obs, tpa, grid, s, A, T);
 }
 
 void launch_force(bool obs, bool kick, int tpa, int grid, cudaStream_t s, AtomsView const &A,
                   TablesView const &T) {
-    if (obs && kick)
-        force_tpa<true, true>(tpa, grid, s, A, T);
-    else if (obs)
-        force_tpa<true, false>(tpa, grid, s, A, T);
-    else if (kick)
-        force_tpa<false, true>(tpa, grid, s, A, T);
+    if (T.interp == MDELAST_BSPLINE)
+        force_ip<MDELAST_BSPLINE>(obs, kick, tpa, grid, s, A, T);
     else
-        force_tpa<false, false>(tpa, grid, s, A, T);
+        force_ip<MDELAST_QUINTIC>(obs, kick, tpa, grid, s, A, T);
 }
 
 } // namespace mdelast

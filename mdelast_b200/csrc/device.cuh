@@ -88,7 +88,7 @@ struct TablesView {
     const double *Ft; // [ntypes][nfi][6]
     int nfi, ntypes;
     double inv_hf, inv_hf2;
-    int has_eam, pad;
+    int has_eam, interp; // interp: MDELAST_QUINTIC or MDELAST_BSPLINE (bundle layout)
     double r_cut_sq; // pow<2>(pot[0]->rcut), md_driver.cpp:42
     double pot_rcut[kMaxTypes * (kMaxTypes + 1) / 2];
     double pot_rmin[kMaxTypes * (kMaxTypes + 1) / 2];
@@ -191,6 +191,46 @@ __device__ __forceinline__ void ld6(const double *p, double c[6]) {
     c[3] = b.y;
     c[4] = d.x;
     c[5] = d.y;
+}
+
+// Interval data of one tabulated function in the two interpolation schemes
+// (poly_table.hpp:137-176): QUINTIC, the 6 coefficients of the quintic in t from which
+// value and derivatives all come (poly_table.hpp:71-97); BSPLINE, 12 = three cubics in t,
+// the pieces of the three independent cubic B-splines through the node values of f, f'
+// and f'' (poly_table.hpp:117-135), evaluated as values. kF is the per-function stride;
+// a pair-table bundle holds three functions (phi_ab, rho_a, rho_b).
+template <int IP> struct TabFmt {
+    static constexpr int kF = IP == MDELAST_BSPLINE ? 12 : 6;
+};
+
+__device__ __forceinline__ double cubic_at(const double *p, double t) {
+    const double2 *q = reinterpret_cast<const double2 *>(p);
+    double2 const a = __ldg(q), b = __ldg(q + 1);
+    return a.x + t * (a.y + t * (b.x + t * b.y));
+}
+
+// value (NV), first (ND1) and second (ND2) derivative of the function whose interval data
+// start at p; inv_h, inv_h2 scale the quintic's derivatives
+template <int IP, bool NV, bool ND1, bool ND2>
+__device__ __forceinline__ void tab_eval(const double *p, double t, double inv_h, double inv_h2,
+                                         double &v, double &d1, double &d2) {
+    if constexpr (IP == MDELAST_BSPLINE) {
+        if (NV)
+            v = cubic_at(p, t);
+        if (ND1)
+            d1 = cubic_at(p + 4, t);
+        if (ND2)
+            d2 = cubic_at(p + 8, t);
+    } else {
+        double c[6];
+        ld6(p, c);
+        if (NV)
+            v = tab_v(c, t);
+        if (ND1)
+            d1 = tab_d1(c, t, inv_h);
+        if (ND2)
+            d2 = tab_d2(c, t, inv_h2);
+    }
 }
 
 } // namespace mdelast

@@ -619,6 +619,9 @@ static int check_config(mdelast_driver_config const &c, mdelast_driver_config co
                         "the GPU path; tabulate them as TablePotential");
         if (p->table.n != p0->table.n || p->table.h != p0->table.h)
             return fail(MDELAST_ERR_UNSUPPORTED, "pair tables on different grids");
+        if (p->interpolation != p0->interpolation)
+            return fail(MDELAST_ERR_UNSUPPORTED,
+                        "pair tables with different interpolations ('quintic', 'bspline')");
     }
     for (int t = 0; t < c.n_eam; ++t) {
         mdelast_eam const *e = c.eam[t];
@@ -627,6 +630,9 @@ static int check_config(mdelast_driver_config const &c, mdelast_driver_config co
         if (e->rho.n != p0->table.n || e->rho.h != p0->table.h ||
             e->F.n != c.eam[0]->F.n || e->F.h != c.eam[0]->F.h)
             return fail(MDELAST_ERR_UNSUPPORTED, "EAM tables on different grids");
+        if (e->interpolation != p0->interpolation)
+            return fail(MDELAST_ERR_UNSUPPORTED,
+                        "EAM and pair tables with different interpolations");
     }
     if (r > 0) { // a batch shares the tables, the list settings, the precision and the device
         bool same = c.n_types == c0.n_types && c.n_eam == c0.n_eam &&
@@ -743,29 +749,34 @@ static int create_system(const mdelast_driver_config *cfgs, int n_rep, mdelast_d
     double const rcut = p0->rcut;
     d->r_list = d->neighbors ? rcut * c0.r_skin : rcut;
 
-    // ---- tables: r-table bundles and embedding tables
+    // ---- tables: r-table bundles and embedding tables. Per interval and function, the 6
+    // quintic coefficients, or for "bspline" the 12 coefficients of the three cubics
+    int const interp = p0->interpolation;
+    bool const bsp = interp == MDELAST_BSPLINE;
+    size_t const kF = bsp ? 12 : 6;
+    auto fun = [&](mdelast::QuinticTable const &q, int k) {
+        return (bsp ? q.cub.data() : q.coef.data()) + kF * static_cast<size_t>(k);
+    };
     int const nri = p0->table.n;
-    std::vector<double> rb(static_cast<size_t>(npot) * nri * 18, 0.);
+    std::vector<double> rb(static_cast<size_t>(npot) * nri * 3 * kF, 0.);
     for (int b = 0; b < nt; ++b)
         for (int a = 0; a <= b; ++a) {
             int const s = b * (b + 1) / 2 + a;
             for (int k = 0; k < nri; ++k) {
-                double *o = rb.data() + (static_cast<size_t>(s) * nri + k) * 18;
-                std::memcpy(o, c0.pair[s]->table.coef.data() + 6 * static_cast<size_t>(k),
-                            6 * sizeof(double));
+                double *o = rb.data() + (static_cast<size_t>(s) * nri + k) * 3 * kF;
+                std::memcpy(o, fun(c0.pair[s]->table, k), kF * sizeof(double));
                 if (c0.n_eam) {
-                    std::memcpy(o + 6, c0.eam[a]->rho.coef.data() + 6 * static_cast<size_t>(k),
-                                6 * sizeof(double));
-                    std::memcpy(o + 12, c0.eam[b]->rho.coef.data() + 6 * static_cast<size_t>(k),
-                                6 * sizeof(double));
+                    std::memcpy(o + kF, fun(c0.eam[a]->rho, k), kF * sizeof(double));
+                    std::memcpy(o + 2 * kF, fun(c0.eam[b]->rho, k), kF * sizeof(double));
                 }
             }
         }
     int const nfi = c0.n_eam ? c0.eam[0]->F.n : 1;
-    std::vector<double> Ft(static_cast<size_t>(nt) * nfi * 6, 0.);
+    std::vector<double> Ft(static_cast<size_t>(nt) * nfi * kF, 0.);
     for (int t = 0; t < c0.n_eam; ++t)
-        std::memcpy(Ft.data() + static_cast<size_t>(t) * nfi * 6, c0.eam[t]->F.coef.data(),
-                    sizeof(double) * 6 * nfi);
+        for (int k = 0; k < nfi; ++k)
+            std::memcpy(Ft.data() + (static_cast<size_t>(t) * nfi + k) * kF,
+                        fun(c0.eam[t]->F, k), sizeof(double) * kF);
     TRY(dalloc(&d->d_rb, rb.size()));
     TRY(dalloc(&d->d_Ft, Ft.size()));
     if (cudaMemcpy(d->d_rb, rb.data(), sizeof(double) * rb.size(), cudaMemcpyHostToDevice) ||
@@ -783,6 +794,7 @@ static int create_system(const mdelast_driver_config *cfgs, int n_rep, mdelast_d
     T.inv_hf = c0.n_eam ? c0.eam[0]->F.inv_h : 1.;
     T.inv_hf2 = c0.n_eam ? c0.eam[0]->F.inv_h2 : 1.;
     T.has_eam = c0.n_eam > 0;
+    T.interp = interp;
     T.r_cut_sq = rcut * rcut;
     for (int s = 0; s < npot; ++s) {
         T.pot_rcut[s] = c0.pair[s]->rcut;
@@ -795,11 +807,21 @@ static int create_system(const mdelast_driver_config *cfgs, int n_rep, mdelast_d
     }
     d->precision = c0.precision;
     if (c0.precision == MDELAST_PRECISION_MIXED) {
-        // the r bundles in FP32, angstrom / eV (phi) and angstrom^-3 (rho)
+        // the r bundles in FP32, angstrom / eV (phi) and angstrom^-3 (rho). Quintic
+        // coefficients carry the function's unit (derivatives come with 1/h in angstrom);
+        // the bspline cubics of f' and f'' carry one and two more 1/length
         std::vector<float> rbf(rb.size());
         double const a3 = kAng * kAng * kAng;
-        for (size_t q = 0; q < rb.size(); ++q)
-            rbf[q] = static_cast<float>(rb[q] * ((q % 18) < 6 ? 1. / kEv : a3));
+        for (size_t q = 0; q < rb.size(); ++q) {
+            size_t const w = q % (3 * kF);
+            double f = w < kF ? 1. / kEv : a3;
+            if (bsp) {
+                int const deriv = static_cast<int>((w % kF) / 4); // 0 f, 1 f', 2 f''
+                for (int d = 0; d < deriv; ++d)
+                    f *= kAng;
+            }
+            rbf[q] = static_cast<float>(rb[q] * f);
+        }
         TRY(dalloc(&d->d_rbf, rbf.size()));
         if (cudaMemcpy(d->d_rbf, rbf.data(), sizeof(float) * rbf.size(), cudaMemcpyHostToDevice))
             return bail(fail(MDELAST_ERR_CUDA, "table upload failed"));
@@ -1527,21 +1549,25 @@ int mdelast_table_eval_device(const mdelast_pair *p, const mdelast_eam *e, int w
     // a one-type table set holding just this function
     mdelast::QuinticTable const &tab = which == 0 ? p->table : (which == 1 ? e->rho : e->F);
     int const nint = tab.n;
+    bool const bsp = tab.bspline != 0;
+    size_t const kF = bsp ? 12 : 6;
+    std::vector<double> const &src = bsp ? tab.cub : tab.coef;
     std::vector<double> rb, Ft;
     TablesView T{};
+    T.interp = bsp ? MDELAST_BSPLINE : MDELAST_QUINTIC;
     if (which == 2) {
-        Ft.assign(tab.coef.begin(), tab.coef.end());
-        rb.assign(18, 0.);
+        Ft.assign(src.begin(), src.end());
+        rb.assign(3 * kF, 0.);
         T.nfi = nint;
         T.inv_hf = tab.inv_h;
         T.inv_hf2 = tab.inv_h2;
         T.nri = 1;
     } else {
-        rb.assign(static_cast<size_t>(nint) * 18, 0.);
+        rb.assign(static_cast<size_t>(nint) * 3 * kF, 0.);
         for (int k = 0; k < nint; ++k)
-            std::memcpy(rb.data() + static_cast<size_t>(k) * 18 + (which == 0 ? 0 : 6),
-                        tab.coef.data() + 6 * static_cast<size_t>(k), 6 * sizeof(double));
-        Ft.assign(6, 0.);
+            std::memcpy(rb.data() + static_cast<size_t>(k) * 3 * kF + (which == 0 ? 0 : kF),
+                        src.data() + kF * static_cast<size_t>(k), kF * sizeof(double));
+        Ft.assign(kF, 0.);
         T.nri = nint;
         T.inv_hr = tab.inv_h;
         T.inv_hr2 = tab.inv_h2;

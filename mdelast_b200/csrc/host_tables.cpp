@@ -62,9 +62,107 @@ int QuinticTable::build(double h_, int64_t n_nodes, double const *f, double cons
     return MDELAST_OK;
 }
 
+namespace {
+
+// Cardinal cubic B-spline through f_0..f_{m-1} on x_i = i h (the Boost 1.84
+// cardinal_cubic_b_spline the reference's BSplineTable uses, restated from the textbook
+// clamped interpolant, de Boor ch. IX): s(x) = sum_k b_k B((x - x_k) / h), k = -1..m, B the
+// centred cubic B-spline, s(x_i) = f_i, end slopes from the second-order one-sided
+// differences, the tridiagonal system solved by the Thomas algorithm. Returns b_-1..b_m.
+std::vector<double> bspline_fit(double h, int m, double const *f) {
+    std::vector<double> out(static_cast<size_t>(m) + 2, m ? f[0] : 0.);
+    if (m < 3)
+        return out;
+    double const inv_h = 1. / h;
+    double const d0 = (-3 * f[0] + 4 * f[1] - f[2]) * inv_h / 2;
+    double const d1 = (3 * f[m - 1] - 4 * f[m - 2] + f[m - 3]) * inv_h / 2;
+    std::vector<double> lo(m, 1.), di(m, 4.), up(m, 1.), rhs(m), b(m);
+    for (int i = 0; i < m; ++i)
+        rhs[i] = 6 * f[i];
+    up[0] = 2;
+    rhs[0] += 2 * h * d0;
+    lo[m - 1] = 2;
+    rhs[m - 1] -= 2 * h * d1;
+    for (int i = 1; i < m; ++i) {
+        double const q = lo[i] / di[i - 1];
+        di[i] -= q * up[i - 1];
+        rhs[i] -= q * rhs[i - 1];
+    }
+    b[m - 1] = rhs[m - 1] / di[m - 1];
+    for (int i = m - 1; i-- > 0;)
+        b[i] = (rhs[i] - up[i] * b[i + 1]) / di[i];
+    for (int i = 0; i < m; ++i)
+        out[static_cast<size_t>(i) + 1] = b[i];
+    out[0] = b[1] - 2 * h * d0;
+    out[static_cast<size_t>(m) + 1] = b[m - 2] + 2 * h * d1;
+    return out;
+}
+
+// the spline's value: the weights of the four nearest coefficients
+double bspline_value(std::vector<double> const &bb, int m, double inv_h, double x) {
+    if (m < 3)
+        return bb[0];
+    double const u = x * inv_h;
+    if (!(u == u))
+        return u;
+    long k = static_cast<long>(std::floor(u));
+    if (k < 0)
+        k = 0;
+    if (k > m - 2)
+        k = m - 2;
+    double s = 0;
+    for (long j = k - 1; j <= k + 2; ++j) {
+        double const t = std::fabs(u - static_cast<double>(j));
+        double w;
+        if (t < 1)
+            w = 2. / 3 - t * t + t * t * t / 2;
+        else if (t < 2)
+            w = (2 - t) * (2 - t) * (2 - t) / 6;
+        else
+            w = 0;
+        s += w * bb[static_cast<size_t>(j + 1)];
+    }
+    return s;
+}
+
+} // namespace
+
+int QuinticTable::build_bspline(double const *f, double const *f1, double const *f2) {
+    int const m = n + 1; // nodes
+    double const *src[3] = {f, f1, f2};
+    for (int q = 0; q < 3; ++q)
+        bs[q] = bspline_fit(h, m, src[q]);
+    // on interval k (t in [0,1)) the spline is the cubic
+    //   ((b_{k-1} + 4 b_k + b_{k+1}) + 3 (b_{k+1} - b_{k-1}) t
+    //    + 3 (b_{k-1} - 2 b_k + b_{k+1}) t^2 + (b_{k+2} - b_{k-1} + 3 (b_k - b_{k+1})) t^3) / 6
+    cub.assign(12 * static_cast<size_t>(n), 0.);
+    using ld = long double;
+    for (int k = 0; k < n; ++k)
+        for (int q = 0; q < 3; ++q) {
+            std::vector<double> const &b = bs[q];
+            ld const bm = b[k], b0 = b[k + 1], b1 = b[k + 2], b2 = b[k + 3];
+            double *c = cub.data() + 12 * static_cast<size_t>(k) + 4 * q;
+            if (m < 3) {
+                c[0] = b[0];
+                continue;
+            }
+            c[0] = static_cast<double>((bm + 4.L * b0 + b1) / 6.L);
+            c[1] = static_cast<double>((b1 - bm) / 2.L);
+            c[2] = static_cast<double>((bm - 2.L * b0 + b1) / 2.L);
+            c[3] = static_cast<double>((b2 - bm + 3.L * (b0 - b1)) / 6.L);
+        }
+    bspline = 1;
+    return MDELAST_OK;
+}
+
 // poly_table.hpp:71-114: interval index clamped to [0, n-1] with the range test done in
 // floating point (a NaN argument takes interval 0 and gives NaN).
 void QuinticTable::eval(double x, double out[3]) const {
+    if (bspline) {
+        for (int q = 0; q < 3; ++q)
+            out[q] = bspline_value(bs[q], n + 1, inv_h, x);
+        return;
+    }
     double const u = x * inv_h;
     int i = 0;
     if (u >= static_cast<double>(n))
@@ -85,12 +183,8 @@ using namespace mdelast;
 namespace {
 
 int check_interp(int interpolation) {
-    if (interpolation == MDELAST_QUINTIC)
+    if (interpolation == MDELAST_QUINTIC || interpolation == MDELAST_BSPLINE)
         return MDELAST_OK;
-    if (interpolation == MDELAST_BSPLINE)
-        return fail(MDELAST_ERR_UNSUPPORTED,
-                    "interpolation 'bspline' (the cubic B-splines of versions <= 1.1) is not "
-                    "implemented on this path; use 'quintic'");
     return fail(MDELAST_ERR_ARGUMENT,
                 "FATAL: unknown table interpolation %d (use 'quintic' or 'bspline')",
                 interpolation);
@@ -115,7 +209,10 @@ int mdelast_pair_table_create(double rcut, double rmin_fatal, double dr, int64_t
     p->interpolation = interpolation;
     p->rcut = rcut;
     p->rmin_fatal = rmin_fatal;
-    if (int rc = p->table.build(dr, n_nodes, v, dv, d2v)) {
+    int rc = p->table.build(dr, n_nodes, v, dv, d2v);
+    if (!rc && interpolation == MDELAST_BSPLINE)
+        rc = p->table.build_bspline(v, dv, d2v);
+    if (rc) {
         delete p;
         return rc;
     }
@@ -213,6 +310,10 @@ int mdelast_eam_create(double rcut, double rhomax_fatal, double dr, double drho,
     int rc = e->rho.build(dr, n_r, rho, drho_dr, d2rho_dr2);
     if (!rc)
         rc = e->F.build(drho, n_rho, F, dF, d2F);
+    if (!rc && interpolation == MDELAST_BSPLINE)
+        rc = e->rho.build_bspline(rho, drho_dr, d2rho_dr2);
+    if (!rc && interpolation == MDELAST_BSPLINE)
+        rc = e->F.build_bspline(F, dF, d2F);
     if (rc) {
         delete e;
         return rc;

@@ -22,8 +22,16 @@ struct QuinticTable {
     int n = 0; // intervals
     std::vector<double> coef; // 6 n
 
+    // "bspline" tables (poly_table.hpp:117-135): three independent cardinal cubic
+    // B-splines through the node values of f, f', f'' (coefficients b_-1..b_n of each), and
+    // per interval the three cubics in t they reduce to (12 n: f, f', f'' pieces)
+    int bspline = 0;
+    std::vector<double> bs[3];
+    std::vector<double> cub;
+
     int build(double h_, int64_t n_nodes, double const *f, double const *f1, double const *f2);
-    // f, f', f'' at x (poly_table.hpp:71-114)
+    int build_bspline(double const *f, double const *f1, double const *f2);
+    // f, f', f'' at x (poly_table.hpp:71-114, or the three splines' values)
     void eval(double x, double out[3]) const;
 };
 

@@ -57,6 +57,36 @@ __device__ __forceinline__ float tabf_d2(const float *c, float t, float inv_h2) 
     return (2.f * c[2] + t * (6.f * c[3] + t * (12.f * c[4] + t * 20.f * c[5]))) * inv_h2;
 }
 
+// FP32 counterpart of tab_eval (device.cuh): QUINTIC interval data are the 6 quintic
+// coefficients, BSPLINE data three cubics (values of the splines of f, f', f''); both with
+// explicit rounding.
+__device__ __forceinline__ float cubicf_at(const float *p, float t) {
+    float4 const a = __ldg(reinterpret_cast<const float4 *>(p));
+    return __fmaf_rn(t, __fmaf_rn(t, __fmaf_rn(t, a.w, a.z), a.y), a.x);
+}
+
+template <int IP, bool NV, bool ND1, bool ND2>
+__device__ __forceinline__ void tabf_eval(const float *p, float t, float inv_h, float inv_h2,
+                                          float &v, float &d1, float &d2) {
+    if constexpr (IP == MDELAST_BSPLINE) {
+        if (NV)
+            v = cubicf_at(p, t);
+        if (ND1)
+            d1 = cubicf_at(p + 4, t);
+        if (ND2)
+            d2 = cubicf_at(p + 8, t);
+    } else {
+        float c[6];
+        ld6f(p, c);
+        if (NV)
+            v = tabf_v(c, t);
+        if (ND1)
+            d1 = tabf_d1(c, t, inv_h);
+        if (ND2)
+            d2 = tabf_d2(c, t, inv_h2);
+    }
+}
+
 // minimum image of pi - pj in a box of edges L (positions wrapped into [-L/2, L/2))
 __device__ __forceinline__ float min_image_f(float4 pi, float4 pj, float3 L, float3 iL,
                                              float &dx, float &dy, float &dz) {
@@ -108,8 +138,9 @@ __device__ __forceinline__ void warp_accumulate(double v, double *slot) {
 // accumulators instead of being carried in registers through the pair loop: the loop then
 // runs with about half the registers, so twice the warps per SM hide the latency of the
 // partner gathers.
-template <bool OBS, int TPA>
+template <bool OBS, int TPA, int IP>
 __global__ void __launch_bounds__(kBlock) k_density_mx(AtomsView A, TablesView T) {
+    constexpr int kF = TabFmt<IP>::kF;
     __shared__ double sacc[kBlock / 32][D_NSUM];
     int const warp = threadIdx.x >> 5;
     for (int k = threadIdx.x; k < (kBlock / 32) * D_NSUM; k += kBlock)
@@ -151,12 +182,14 @@ __global__ void __launch_bounds__(kBlock) k_density_mx(AtomsView A, TablesView T
                     continue;
                 float t;
                 int const k = tab_locate_f(dr, T.finv_hr, T.nri, t);
-                int const off = (tj == (ti < tj ? ti : tj)) ? 6 : 12;
-                float c[6];
-                ld6f(T.rbf + (static_cast<size_t>(pair_slot(ti, tj)) * T.nri + k) * 18 + off, c);
-                rho += tabf_v(c, t);
+                int const off = (tj == (ti < tj ? ti : tj)) ? kF : 2 * kF;
+                float v = 0.f, d1 = 0.f, d2 = 0.f;
+                tabf_eval<IP, true, OBS, false>(
+                    T.rbf + (static_cast<size_t>(pair_slot(ti, tj)) * T.nri + k) * 3 * kF + off,
+                    t, T.finv_hr, T.finv_hr2, v, d1, d2);
+                rho += v;
                 if (OBS) {
-                    float const ar = tabf_d1(c, t, T.finv_hr) * idr;
+                    float const ar = d1 * idr;
                     float const ap[3] = {ar * dx, ar * dy, ar * dz};
                     g[0] += ap[0] * dx;
                     g[1] += ap[1] * dy;
@@ -188,11 +221,9 @@ __global__ void __launch_bounds__(kBlock) k_density_mx(AtomsView A, TablesView T
                 status_or(A.rep + r, MDELAST_FATAL_RHO_MAX);
             double t;
             int const k = tab_locate(rc, T.inv_hf, T.nfi, t);
-            double c[6];
-            ld6(T.Ft + (static_cast<size_t>(ti) * T.nfi + k) * 6, c);
-            F = tab_v(c, t);
-            double const dF = tab_d1(c, t, T.inv_hf);
-            d2F = OBS ? tab_d2(c, t, T.inv_hf2) : 0.;
+            double dF = 0.;
+            tab_eval<IP, true, true, OBS>(T.Ft + (static_cast<size_t>(ti) * T.nfi + k) * kF, t,
+                                          T.inv_hf, T.inv_hf2, F, dF, d2F);
             A.rho[i] = rc;
             A.Fe[i] = F;
             // F' [erg cm^3] -> [eV A^3] and F'' [erg cm^6] -> [eV A^6]
@@ -260,7 +291,7 @@ struct RowIn {
 // One lane's walk over list slots [s0, s1) of an atom row (slots of partners j > i when
 // UPPER, else of partners j < i, addressed from the end of the row); every pair adds its
 // force and half its energy to the atom, and pairs j > i also add to the global sums.
-template <bool OBS, bool UPPER, int TPA>
+template <bool OBS, bool UPPER, int TPA, int IP>
 __device__ __forceinline__ void force_row_mx(AtomsView const &A, TablesView const &T,
                                              RowIn const &in, const int *row, int n, int sub,
                                              double &fx, double &fy, double &fz, double &epot,
@@ -290,40 +321,27 @@ __device__ __forceinline__ void force_row_mx(AtomsView const &A, TablesView cons
         int const s = pair_slot(ti, tj);
         float t;
         int const k = tab_locate_f(dr, T.finv_hr, T.nri, t);
-        const float *bundle = T.rbf + (static_cast<size_t>(s) * T.nri + k) * 18;
+        constexpr int kF = TabFmt<IP>::kF;
+        const float *bundle = T.rbf + (static_cast<size_t>(s) * T.nri + k) * 3 * kF;
         float V = 0.f, dV = 0.f, d2V = 0.f;
         if (dr < T.fpot_rmin[s])
             warn_rmin = true;
-        if (!(dr > T.fpot_rcut[s])) {
-            float c[6];
-            ld6f(bundle, c);
-            V = tabf_v(c, t);
-            dV = tabf_d1(c, t, T.finv_hr);
-            if (OBS)
-                d2V = tabf_d2(c, t, T.finv_hr2);
-        }
+        if (!(dr > T.fpot_rcut[s]))
+            tabf_eval<IP, true, true, OBS>(bundle, t, T.finv_hr, T.finv_hr2, V, dV, d2V);
         float dedr = dV, X = 0.f, lap = 0.f;
         if (OBS) {
             X = d2V - dV * idr;
             lap = 2.f * (d2V + 2.f * dV * idr);
         }
         if (T.has_eam) {
-            int const oi = (ti <= tj) ? 6 : 12, oj = (ti < tj) ? 12 : 6;
-            float drho_i = 0.f, drho_j = 0.f, d2rho_i = 0.f, d2rho_j = 0.f;
-            if (!(dr > T.feam_rcut[ti])) {
-                float c[6];
-                ld6f(bundle + oi, c);
-                drho_i = tabf_d1(c, t, T.finv_hr);
-                if (OBS)
-                    d2rho_i = tabf_d2(c, t, T.finv_hr2);
-            }
-            if (!(dr > T.feam_rcut[tj])) {
-                float c[6];
-                ld6f(bundle + oj, c);
-                drho_j = tabf_d1(c, t, T.finv_hr);
-                if (OBS)
-                    d2rho_j = tabf_d2(c, t, T.finv_hr2);
-            }
+            int const oi = (ti <= tj) ? kF : 2 * kF, oj = (ti < tj) ? 2 * kF : kF;
+            float drho_i = 0.f, drho_j = 0.f, d2rho_i = 0.f, d2rho_j = 0.f, unused = 0.f;
+            if (!(dr > T.feam_rcut[ti]))
+                tabf_eval<IP, false, true, OBS>(bundle + oi, t, T.finv_hr, T.finv_hr2, unused,
+                                                drho_i, d2rho_i);
+            if (!(dr > T.feam_rcut[tj]))
+                tabf_eval<IP, false, true, OBS>(bundle + oj, t, T.finv_hr, T.finv_hr2, unused,
+                                                drho_j, d2rho_j);
             float const dFj = dFj2.x, dFi = in.dFi;
             // the two cross terms rounded separately and added commutatively: the pair
             // force is the same, bit for bit, seen from either atom
@@ -380,7 +398,7 @@ __device__ __forceinline__ void force_row_mx(AtomsView const &A, TablesView cons
 // (which also feed the global sums) and partners j < i, so the lanes of a warp do not
 // diverge on the global-sum work. The per-thread FP64 block accumulators live in shared
 // memory (slot-major) rather than registers.
-template <bool OBS, bool KICK, int TPA>
+template <bool OBS, bool KICK, int TPA, int IP>
 __global__ void __launch_bounds__(kBlock) k_force_mx(AtomsView A, TablesView T) {
     __shared__ double s_acc[F_NSUM * kBlock];
     int const tid = threadIdx.x;
@@ -410,10 +428,10 @@ __global__ void __launch_bounds__(kBlock) k_force_mx(AtomsView A, TablesView T) 
             int const *row = A.nbr + static_cast<size_t>(i) * A.maxn;
             bool warn_rmin = false;
             PairSums<OBS> ps;
-            force_row_mx<OBS, true, TPA>(A, T, in, row, nu, sub, fx, fy, fz, epot, ps,
-                                         warn_rmin);
-            force_row_mx<OBS, false, TPA>(A, T, in, row, nd, sub, fx, fy, fz, epot, ps,
-                                          warn_rmin);
+            force_row_mx<OBS, true, TPA, IP>(A, T, in, row, nu, sub, fx, fy, fz, epot, ps,
+                                             warn_rmin);
+            force_row_mx<OBS, false, TPA, IP>(A, T, in, row, nd, sub, fx, fy, fz, epot, ps,
+                                              warn_rmin);
             if (warn_rmin)
                 status_or(A.rep + r, MDELAST_WARN_RMIN);
             s_acc[F_VIRIAL * kBlock + tid] += (ps.sig_d[0] + ps.sig_d[1]) + ps.sig_d[2];
@@ -489,44 +507,60 @@ __global__ void __launch_bounds__(kBlock) k_force_mx(AtomsView A, TablesView T) 
 }
 
 namespace {
-template <bool OBS>
+template <bool OBS, int IP>
 void density_mx_tpa(int tpa, int grid, cudaStream_t s, AtomsView const &A, TablesView const &T) {
     switch (tpa) {
-    case 1: k_density_mx<OBS, 1><<<grid, kBlock, 0, s>>>(A, T); break;
-    case 4: k_density_mx<OBS, 4><<<grid, kBlock, 0, s>>>(A, T); break;
-    case 8: k_density_mx<OBS, 8><<<grid, kBlock, 0, s>>>(A, T); break;
-    default: k_density_mx<OBS, 16><<<grid, kBlock, 0, s>>>(A, T); break;
+    case 1: k_density_mx<OBS, 1, IP><<<grid, kBlock, 0, s>>>(A, T); break;
+    case 4: k_density_mx<OBS, 4, IP><<<grid, kBlock, 0, s>>>(A, T); break;
+    case 8: k_density_mx<OBS, 8, IP><<<grid, kBlock, 0, s>>>(A, T); break;
+    default: k_density_mx<OBS, 16, IP><<<grid, kBlock, 0, s>>>(A, T); break;
     }
 }
-template <bool OBS, bool KICK>
+template <bool OBS, bool KICK, int IP>
 void force_mx_tpa(int tpa, int grid, cudaStream_t s, AtomsView const &A, TablesView const &T) {
     switch (tpa) {
-    case 1: k_force_mx<OBS, KICK, 1><<<grid, kBlock, 0, s>>>(A, T); break;
-    case 4: k_force_mx<OBS, KICK, 4><<<grid, kBlock, 0, s>>>(A, T); break;
-    case 8: k_force_mx<OBS, KICK, 8><<<grid, kBlock, 0, s>>>(A, T); break;
-    default: k_force_mx<OBS, KICK, 16><<<grid, kBlock, 0, s>>>(A, T); break;
+    case 1: k_force_mx<OBS, KICK, 1, IP><<<grid, kBlock, 0, s>>>(A, T); break;
+    case 4: k_force_mx<OBS, KICK, 4, IP><<<grid, kBlock, 0, s>>>(A, T); break;
+    case 8: k_force_mx<OBS, KICK, 8, IP><<<grid, kBlock, 0, s>>>(A, T); break;
+    default: k_force_mx<OBS, KICK, 16, IP><<<grid, kBlock, 0, s>>>(A, T); break;
     }
+}
+template <int IP>
+void density_mx_ip(bool obs, int tpa, int grid, cudaStream_t s, AtomsView const &A,
+                   TablesView const &T) {
+    if (obs)
+        density_mx_tpa<true, IP>(tpa, grid, s, A, T);
+    else
+        density_mx_tpa<false, IP>(tpa, grid, s, A, T);
+}
+template <int IP>
+void force_mx_ip(bool obs, bool kick, int tpa, int grid, cudaStream_t s, AtomsView const &A,
+                 TablesView const &T) {
+    if (obs && kick)
+        force_mx_tpa<true, true, IP>(tpa, grid, s, A, T);
+    else if (obs)
+        force_mx_tpa<true, false, IP>(tpa, grid, s, A, T);
+    else if (kick)
+        force_mx_tpa<false, true, IP>(tpa, grid, s, A, T);
+    else
+        force_mx_tpa<false, false, IP>(tpa, grid, s, A, T);
 }
 } // namespace
 
 void launch_density_mx(bool obs, int tpa, int grid, cudaStream_t s, AtomsView const &A,
                        TablesView const &T) {
-    if (obs)
-        density_mx_tpa<true>(tpa, grid, s, A, T);
+    if (T.interp == MDELAST_BSPLINE)
+        density_mx_ip<MDELAST_BSPLINE>(obs, tpa, grid, s, A, T);
     else
-        density_mx_tpa<false>(tpa, grid, s, A, T);
+        density_mx_ip<MDELAST_QUINTIC>(obs, tpa, grid, s, A, T);
 }
 
 void launch_force_mx(bool obs, bool kick, int tpa, int grid, cudaStream_t s, AtomsView const &A,
                      TablesView const &T) {
-    if (obs && kick)
-        force_mx_tpa<true, true>(tpa, grid, s, A, T);
-    else if (obs)
-        force_mx_tpa<true, false>(tpa, grid, s, A, T);
-    else if (kick)
-        force_mx_tpa<false, true>(tpa, grid, s, A, T);
+    if (T.interp == MDELAST_BSPLINE)
+        force_mx_ip<MDELAST_BSPLINE>(obs, kick, tpa, grid, s, A, T);
     else
-        force_mx_tpa<false, false>(tpa, grid, s, A, T);
+        force_mx_ip<MDELAST_QUINTIC>(obs, kick, tpa, grid, s, A, T);
 }
 
 } // namespace mdelast

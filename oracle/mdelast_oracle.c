@@ -35,7 +35,95 @@ typedef struct {
     double h, inv_h, inv_h2;
     int n; /* intervals */
     double *c; /* 6 per interval */
+    /* "bspline" (poly_table.hpp:117-135): three cardinal cubic B-splines through the node
+     * values of f, f', f''; coefficients b_{-1}..b_{n_nodes} of each, NULL for quintic */
+    double *bs[3];
+    int nodes;
 } qtab;
+
+/* Cardinal cubic B-spline on nodes x_i = i h, i < n (Boost 1.84
+ * cardinal_cubic_b_spline, which the reference uses for its "bspline" tables; restated
+ * here, and in the project's shim oracle/shim/boost/.../cardinal_cubic_b_spline.hpp, from
+ * the textbook clamped interpolant, de Boor ch. IX): s(x) = sum_k b_k B((x - x_k) / h),
+ * k = -1..n, B the centred cubic B-spline, s(x_i) = f_i, and the end slopes estimated by the
+ * second-order one-sided differences. Same operations, in the same order, as the shim. */
+static void bspline_fit(double h, int n, double const *f, double *b_out /* n + 2 */) {
+    double const inv_h = 1. / h;
+    if (n < 3) {
+        for (int i = 0; i < n + 2; ++i)
+            b_out[i] = n ? f[0] : 0.;
+        return;
+    }
+    double const d0 = (-3 * f[0] + 4 * f[1] - f[2]) * inv_h / 2;
+    double const d1 = (3 * f[n - 1] - 4 * f[n - 2] + f[n - 3]) * inv_h / 2;
+    double *lo = (double *)malloc(sizeof(double) * (size_t)n);
+    double *di = (double *)malloc(sizeof(double) * (size_t)n);
+    double *up = (double *)malloc(sizeof(double) * (size_t)n);
+    double *rhs = (double *)malloc(sizeof(double) * (size_t)n);
+    double *b = (double *)malloc(sizeof(double) * (size_t)n);
+    for (int i = 0; i < n; ++i) {
+        lo[i] = 1;
+        di[i] = 4;
+        up[i] = 1;
+        rhs[i] = 6 * f[i];
+    }
+    up[0] = 2;
+    rhs[0] += 2 * h * d0;
+    lo[n - 1] = 2;
+    rhs[n - 1] -= 2 * h * d1;
+    for (int i = 1; i < n; ++i) {
+        double const m = lo[i] / di[i - 1];
+        di[i] -= m * up[i - 1];
+        rhs[i] -= m * rhs[i - 1];
+    }
+    b[n - 1] = rhs[n - 1] / di[n - 1];
+    for (int i = n - 1; i-- > 0;)
+        b[i] = (rhs[i] - up[i] * b[i + 1]) / di[i];
+    for (int i = 0; i < n; ++i)
+        b_out[i + 1] = b[i];
+    b_out[0] = b[1] - 2 * h * d0;
+    b_out[n + 1] = b[n - 2] + 2 * h * d1;
+    free(lo);
+    free(di);
+    free(up);
+    free(rhs);
+    free(b);
+}
+
+static double bspline_eval(double const *bb, int n, double inv_h, double x) {
+    if (n < 3)
+        return bb[0];
+    double const u = (x - 0.) * inv_h;
+    long k = (long)floor(u);
+    if (!(u == u))
+        return u;
+    if (k < 0)
+        k = 0;
+    if (k > (long)n - 2)
+        k = (long)n - 2;
+    double s = 0;
+    for (long j = k - 1; j <= k + 2; ++j) {
+        double const t = fabs(u - (double)j);
+        double w;
+        if (t < 1)
+            w = 2. / 3 - t * t + t * t * t / 2;
+        else if (t < 2)
+            w = (2 - t) * (2 - t) * (2 - t) / 6;
+        else
+            w = 0;
+        s += w * bb[j + 1];
+    }
+    return s;
+}
+
+/* the spline through f_0..f_{n-1} (spacing h) evaluated at x: a test entry point */
+double orc_bspline_value(double h, int n, double const *f, double x) {
+    double *b = (double *)malloc(sizeof(double) * ((size_t)n + 2));
+    bspline_fit(h, n, f, b);
+    double const v = bspline_eval(b, n, 1. / h, x);
+    free(b);
+    return v;
+}
 
 int orc_quintic_coefficients(double h, int n_nodes, double const *f, double const *f1,
                              double const *f2, double *coef) {
@@ -62,13 +150,28 @@ int orc_quintic_coefficients(double h, int n_nodes, double const *f, double cons
 }
 
 static int qtab_init(qtab *t, double h, int n_nodes, double const *f, double const *f1,
-                     double const *f2) {
+                     double const *f2, int bspline) {
     t->h = h;
     t->inv_h = 1. / h;
     t->inv_h2 = 1. / (h * h);
     t->n = n_nodes - 1;
+    t->nodes = n_nodes;
     t->c = (double *)malloc(sizeof(double) * 6 * (size_t)(t->n > 0 ? t->n : 1));
+    t->bs[0] = t->bs[1] = t->bs[2] = NULL;
+    if (bspline) {
+        double const *src[3] = {f, f1, f2};
+        for (int k = 0; k < 3; ++k) {
+            t->bs[k] = (double *)malloc(sizeof(double) * ((size_t)n_nodes + 2));
+            bspline_fit(h, n_nodes, src[k], t->bs[k]);
+        }
+    }
     return orc_quintic_coefficients(h, n_nodes, f, f1, f2, t->c);
+}
+
+static void qtab_free(qtab *t) {
+    free(t->c);
+    for (int k = 0; k < 3; ++k)
+        free(t->bs[k]);
 }
 
 /* poly_table.hpp:105-114: clamped interval index, NaN-safe */
@@ -84,12 +187,16 @@ static double const *qtab_locate(qtab const *T, double x, double *t) {
 }
 
 static double qtab_value(qtab const *T, double x) {
+    if (T->bs[0])
+        return bspline_eval(T->bs[0], T->nodes, T->inv_h, x);
     double t;
     double const *c = qtab_locate(T, x, &t);
     return c[0] + t * (c[1] + t * (c[2] + t * (c[3] + t * (c[4] + t * c[5]))));
 }
 
 static double qtab_d1(qtab const *T, double x) {
+    if (T->bs[1])
+        return bspline_eval(T->bs[1], T->nodes, T->inv_h, x);
     double t;
     double const *c = qtab_locate(T, x, &t);
     return (c[1] + t * (2. * c[2] + t * (3. * c[3] + t * (4. * c[4] + t * 5. * c[5])))) *
@@ -97,13 +204,16 @@ static double qtab_d1(qtab const *T, double x) {
 }
 
 static double qtab_d2(qtab const *T, double x) {
+    if (T->bs[2])
+        return bspline_eval(T->bs[2], T->nodes, T->inv_h, x);
     double t;
     double const *c = qtab_locate(T, x, &t);
     return (2. * c[2] + t * (6. * c[3] + t * (12. * c[4] + t * 20. * c[5]))) * T->inv_h2;
 }
 
 void orc_quintic_eval(double const *coef, int n_intervals, double h, double x, double *o) {
-    qtab T = {h, 1. / h, 1. / (h * h), n_intervals, (double *)coef};
+    qtab T = {h, 1. / h, 1. / (h * h), n_intervals, (double *)coef, {NULL, NULL, NULL},
+              n_intervals + 1};
     o[0] = qtab_value(&T, x);
     o[1] = qtab_d1(&T, x);
     o[2] = qtab_d2(&T, x);
@@ -672,7 +782,8 @@ orc_system *orc_create(int n_types, char const *interpolation, double rcut, doub
                        int nchain_b, double const *qb, double const *p_eta_b, double Nf_b,
                        double const *box9, int n_rg, double const *rg, double Nf, double dt,
                        int neighbors, double r_skin, double fatal_conservation) {
-    if (strcmp(interpolation, "quintic") != 0)
+    int const bspline = strcmp(interpolation, "bspline") == 0;
+    if (!bspline && strcmp(interpolation, "quintic") != 0)
         return NULL;
     orc_system *s = (orc_system *)calloc(1, sizeof(orc_system));
     int const N = n_atoms;
@@ -687,15 +798,15 @@ orc_system *orc_create(int n_types, char const *interpolation, double rcut, doub
     s->pot = (qtab *)calloc((size_t)s->npot, sizeof(qtab));
     for (int k = 0; k < s->npot; ++k)
         qtab_init(&s->pot[k], dr, n_r, phi + (long)k * n_r, dphi + (long)k * n_r,
-                  d2phi + (long)k * n_r);
+                  d2phi + (long)k * n_r, bspline);
     s->trho = (qtab *)calloc((size_t)n_types, sizeof(qtab));
     s->tF = (qtab *)calloc((size_t)n_types, sizeof(qtab));
     if (has_eam) {
         for (int t = 0; t < n_types; ++t) {
             qtab_init(&s->trho[t], dr, n_r, rho + (long)t * n_r, drho_dr + (long)t * n_r,
-                      d2rho_dr2 + (long)t * n_r);
+                      d2rho_dr2 + (long)t * n_r, bspline);
             qtab_init(&s->tF[t], drho, n_rho, F + (long)t * n_rho, dF + (long)t * n_rho,
-                      d2F + (long)t * n_rho);
+                      d2F + (long)t * n_rho, bspline);
         }
     }
     s->mass = dup(mass, n_types);
@@ -772,10 +883,10 @@ void orc_destroy(orc_system *s) {
     if (!s)
         return;
     for (int k = 0; k < s->npot; ++k)
-        free(s->pot[k].c);
+        qtab_free(&s->pot[k]);
     for (int t = 0; t < s->ntypes; ++t) {
-        free(s->trho[t].c);
-        free(s->tF[t].c);
+        qtab_free(&s->trho[t]);
+        qtab_free(&s->tF[t]);
     }
     free(s->pot);
     free(s->trho);

@@ -53,6 +53,7 @@ void orc_gr(orc_system const *s, double *gr, double *gr_partial);
  * intervals, 6 per interval, built in long double. */
 int orc_quintic_coefficients(double h, int n_nodes, double const *f, double const *f1,
                              double const *f2, double *coef_out);
+double orc_bspline_value(double h, int n, double const *f, double x);
 void orc_quintic_eval(double const *coef, int n_intervals, double h, double x, double *out3);
 
 /* status bits, the same meaning as the MDELAST_STATUS_* bits of include/mdelast.h */

@@ -45,6 +45,7 @@ class Case:
     neighbors: bool = False
     r_skin: float = 1.0
     fatal_conservation: float = 1e3
+    interpolation: str = "quintic"
 
     @property
     def N(self):
@@ -78,13 +79,14 @@ def oracle(case: Case, which="oracle"):
     from oracle.ref import OracleDriver, RefDriver
     cls = OracleDriver if which == "oracle" else RefDriver
     with quiet_fd1():
-        return cls(case.tables, case.positions, case.velocities, case.types, **case.kw())
+        return cls(case.tables, case.positions, case.velocities, case.types,
+                   interpolation=case.interpolation, **case.kw())
 
 
 def gpu(case: Case, precision="fp64"):
     import md_driver_module as m
     t = case.tables
-    _, pots, eams = make_objects(m, t)
+    _, pots, eams = make_objects(m, t, case.interpolation)
     P = [m.Vector3d(*p) for p in case.positions]
     V = [m.Vector3d(*v) for v in case.velocities]
     T, q, p_eta, nf = case.thermo

@@ -117,3 +117,24 @@ def test_no_device_no_fallback(lib):
     from helpers import gpu, static_case
     with pytest.raises(RuntimeError, match="no CUDA device"):
         gpu(static_case())
+
+
+def test_bspline_table_matches_oracle(lib):
+    """"bspline" tables (poly_table.hpp:117-135): the host evaluator (Potential.calculate)
+    gives the oracle's three spline values bit for bit."""
+    D = C.POINTER(C.c_double)
+    rng = np.random.RandomState(4)
+    n, h = 57, 0.0021
+    fs = [rng.normal(size=n) for _ in range(3)]
+    rc, p = _pair(lib, h, *fs, interp=1)
+    assert rc == 0
+    orc = C.CDLL(ORACLE)
+    orc.orc_bspline_value.argtypes = [C.c_double, C.c_int, D, C.c_double]
+    orc.orc_bspline_value.restype = C.c_double
+    lib.mdelast_pair_eval.argtypes = [C.c_void_p, C.c_double, D]
+    for x in np.concatenate([np.linspace(0.0, (n - 1) * h, 613), [0.5 * h, 3 * h]]):
+        a = np.zeros(3)
+        assert lib.mdelast_pair_eval(p, x, a.ctypes.data_as(D)) == 0
+        b = [orc.orc_bspline_value(h, n, f.ctypes.data_as(D), x) for f in fs]
+        assert np.array_equal(a, b), x
+    lib.mdelast_pair_destroy(p)

@@ -126,3 +126,29 @@ def test_oracle_bitwise_l12():
     a.integrate(5)
     b.integrate(5)
     assert np.array_equal(a.scalars(), b.scalars())
+
+
+@needs_ref
+@pytest.mark.parametrize("which", ["ref", "oracle"])
+def test_bspline_static_golden(which):
+    """Benchmark S Part A6 with the "bspline" tables of versions <= 1.1 (smoke.json:34-88,
+    bspline column) within its rel 1e-7: the compiled reference through the project's
+    cubic B-spline shim, and the C restatement."""
+    from dataclasses import replace
+    vals = a6_values(oracle(replace(static_case(), interpolation="bspline"), which))
+    for k, v in vals.items():
+        assert abs(v / GOLD["bspline"][k] - 1.0) < GOLD["rel_tol"], k
+
+
+@needs_ref
+@needs_oracle
+@pytest.mark.parametrize("maker", ["static", "npt"])
+def test_oracle_bitwise_bspline(maker):
+    from dataclasses import replace
+    c = static_case() if maker == "static" else dynamics_case(nside=4, n_zn=15, ensemble=2)
+    c = replace(c, interpolation="bspline")
+    a, b = oracle(c, "ref"), oracle(c, "oracle")
+    a.integrate(10)
+    b.integrate(10)
+    assert np.array_equal(a.scalars(), b.scalars())
+    assert np.array_equal(a.atoms("forces"), b.atoms("forces"))
