@@ -281,6 +281,15 @@ int mdelast_driver_autotune(mdelast_driver *d, int32_t n_repeat, int32_t *choice
                             double *ms_out);
 int mdelast_driver_set_launch(mdelast_driver *d, int32_t tpa_density, int32_t tpa_force,
                               int32_t blocks_density, int32_t blocks_force);
+/* The list the pair passes walk. No counterpart in the reference (its passes walk the
+ * neighbour list, whose pairs beyond r_cut they skip). factor > 1: the neighbour list's
+ * pairs within factor * r_cut (FP64 min-image, the same test from both atoms), rebuilt after
+ * every neighbour-list rebuild and whenever some atom has moved by more than
+ * (factor - 1) r_cut / 2 since the last refresh, so every pair within r_cut is kept and the
+ * results do not change; factor 0: the neighbour list itself. Drivers start at 1.06 when
+ * they keep a neighbour list with r_skin above it (the environment variable
+ * MDELAST_PAIR_LIST sets another start value). */
+int mdelast_driver_set_pair_list(mdelast_driver *d, double factor);
 
 /* ---- Samples and fluctuation sums (molecular_dynamics.py:1218-1238, 663-1000) ----
  *

@@ -191,14 +191,14 @@ __global__ void __launch_bounds__(kBlock) k_density(AtomsView A, TablesView T) {
     if (valid) {
         ci = A.crd[i];
         int const ti = static_cast<int>(ci.w);
-        int const nu = A.n_up[i], ntot = nu + A.n_dn[i];
-        int const *row = A.nbr + static_cast<size_t>(i) * A.maxn;
+        int const nu = A.pn_up[i], ntot = nu + A.pn_dn[i];
+        int const *row = A.pnbr + static_cast<size_t>(i) * A.pmaxn;
         // the next partner's index and record are loaded one iteration ahead
-        double4 cn = A.crd[sub < ntot ? row[list_slot(sub, nu, A.maxn)] : i];
+        double4 cn = A.crd[sub < ntot ? row[list_slot(sub, nu, A.pmaxn)] : i];
         for (int kk = sub; kk < ntot; kk += TPA) {
             double4 const cj = cn;
             if (kk + TPA < ntot)
-                cn = A.crd[row[list_slot(kk + TPA, nu, A.maxn)]];
+                cn = A.crd[row[list_slot(kk + TPA, nu, A.pmaxn)]];
             double px, py, pz;
             double const r2 = min_image_r2(ci, cj, hx, hy, hz, px, py, pz);
             if (r2 > T.r_cut_sq)
@@ -303,11 +303,11 @@ __global__ void __launch_bounds__(kBlock) k_force(AtomsView A, TablesView T) {
         int const ti = static_cast<int>(ci.w);
         double2 const dFi2 = T.has_eam ? A.dF2[i] : make_double2(0., 0.);
         double const dFi = dFi2.x, d2Fi = OBS ? dFi2.y : 0.;
-        int const nu = A.n_up[i], ntot = nu + A.n_dn[i];
-        int const *row = A.nbr + static_cast<size_t>(i) * A.maxn;
+        int const nu = A.pn_up[i], ntot = nu + A.pn_dn[i];
+        int const *row = A.pnbr + static_cast<size_t>(i) * A.pmaxn;
         bool warn_rmin = false;
         // the next partner's index, record and F' are loaded one iteration ahead
-        int jn = sub < ntot ? row[list_slot(sub, nu, A.maxn)] : i;
+        int jn = sub < ntot ? row[list_slot(sub, nu, A.pmaxn)] : i;
         double4 cn = A.crd[jn];
         double2 fn = A.dF2[jn];
         for (int kk = sub; kk < ntot; kk += TPA) {
@@ -315,7 +315,7 @@ __global__ void __launch_bounds__(kBlock) k_force(AtomsView A, TablesView T) {
             double4 const cj = cn;
             double2 const dFj2 = fn;
             if (kk + TPA < ntot) {
-                jn = row[list_slot(kk + TPA, nu, A.maxn)];
+                jn = row[list_slot(kk + TPA, nu, A.pmaxn)];
                 cn = A.crd[jn];
                 fn = A.dF2[jn];
             }
@@ -454,12 +454,12 @@ __global__ void __launch_bounds__(kBlock) k_force(AtomsView A, TablesView T) {
 // c += (cf dt) v / h with the box before this step's barostat update.
 
 __global__ void __launch_bounds__(kBlock) k_kick_drift(AtomsView A, TablesView T) {
+    // the grid covers the n_pad slots exactly; a warp never spans two replicas (their
+    // ranges start on multiples of kTile) and its padding slots, if any, come last
     int const i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= A.n_pad)
-        return;
     int const r = A.rep_of[i];
-    if (r < 0)
-        return;
+    double d2 = 0.;
+    if (r >= 0) {
     Replica const *R = A.rep + r;
     size_t const np = A.n_pad;
     double4 c = A.crd[i];
@@ -477,11 +477,87 @@ __global__ void __launch_bounds__(kBlock) k_kick_drift(AtomsView A, TablesView T
     c.y = __dadd_rn(c.y, __ddiv_rn(__dmul_rn(a, v[1]), R->h_pos[1]));
     c.z = __dadd_rn(c.z, __ddiv_rn(__dmul_rn(a, v[2]), R->h_pos[2]));
     A.crd[i] = c;
+    if (A.crd_ref) {
+        // squared displacement since the pair list was refreshed (position in this step's
+        // box against the position in the refresh's box)
+        double4 const c0 = A.crd_ref[i];
+        double const dx = c.x * R->h[0] - c0.x, dy = c.y * R->h[1] - c0.y,
+                     dz = c.z * R->h[2] - c0.z;
+        d2 = dx * dx + dy * dy + dz * dz;
+    }
     if (A.posf) // mixed precision: wrapped FP32 positions in the box after this drift
         A.posf[i] = make_float4(static_cast<float>((c.x - nint_ref(c.x)) * R->h[0] / kAng),
                                 static_cast<float>((c.y - nint_ref(c.y)) * R->h[1] / kAng),
                                 static_cast<float>((c.z - nint_ref(c.z)) * R->h[2] / kAng),
                                 static_cast<float>(c.w));
+    }
+    if (A.crd_ref) {
+        // the replica's largest displacement: warp maximum, then one atomic per warp
+        // (non-negative doubles order like their bit patterns)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+            d2 = fmax(d2, __shfl_xor_sync(0xffffffffu, d2, o));
+        int const r0 = __shfl_sync(0xffffffffu, r, 0);
+        if ((threadIdx.x & 31) == 0 && r0 >= 0 && d2 > 0.)
+            atomicMax(reinterpret_cast<unsigned long long *>(&A.rep[r0].sub_d2),
+                      static_cast<unsigned long long>(__double_as_longlong(d2)));
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// Pair list of the pair passes: the pairs of the neighbour list within sub_r2, the same
+// FP64 min-image test on both atoms of a pair (so the list is symmetric), in list order.
+// A replica's rows are rebuilt when its list was rebuilt or when some atom has moved by
+// more than half the radius margin since the last refresh: then every pair now within
+// r_cut is still in the list. One warp per atom slot; the warp takes 32 entries at a time
+// and compacts the kept ones with a ballot.
+
+__global__ void __launch_bounds__(256) k_sublist(AtomsView A) {
+    int const i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int const lane = threadIdx.x & 31;
+    if (i >= A.n_pad)
+        return;
+    int const r = A.rep_of[i];
+    if (r < 0)
+        return;
+    Replica const *R = A.rep + r;
+    if (!(R->sub_force || R->sub_d2 > A.sub_half2))
+        return;
+    double4 const ci = A.crd[i];
+    double const hx = R->h[0], hy = R->h[1], hz = R->h[2];
+    int const nu = A.n_up[i], nd = A.n_dn[i];
+    int const *row = A.nbr + static_cast<size_t>(i) * A.maxn;
+    int *out = A.pnbr + static_cast<size_t>(i) * A.pmaxn;
+    unsigned const lt = (1u << lane) - 1u;
+    int ku = 0, kd = 0;
+    for (int k0 = 0; k0 < nu + nd; k0 += 32) {
+        int const k = k0 + lane;
+        bool keep = false, upper = k < nu;
+        int j = -1;
+        if (k < nu + nd) {
+            j = row[upper ? k : A.maxn - 1 - (k - nu)];
+            double px, py, pz;
+            keep = min_image_r2(ci, A.crd[j], hx, hy, hz, px, py, pz) <= A.sub_r2;
+        }
+        unsigned const bu = __ballot_sync(0xffffffffu, keep && upper);
+        unsigned const bd = __ballot_sync(0xffffffffu, keep && !upper);
+        if (keep && upper)
+            out[ku + __popc(bu & lt)] = j;
+        if (keep && !upper)
+            out[A.pmaxn - 1 - (kd + __popc(bd & lt))] = j;
+        ku += __popc(bu);
+        kd += __popc(bd);
+    }
+    if (lane == 0) {
+        A.pn_up[i] = ku;
+        A.pn_dn[i] = kd;
+        A.crd_ref[i] = make_double4(ci.x * hx, ci.y * hy, ci.z * hz, ci.w);
+    }
+}
+
+__global__ void k_sub_invalidate(AtomsView A) {
+    for (int r = threadIdx.x; r < A.n_rep; r += blockDim.x)
+        A.rep[r].sub_force = 1;
 }
 
 // ------------------------------------------------------------------------------------

@@ -79,6 +79,10 @@ struct Replica {
     double n_samples;
     int acc_on, pad3;
     mdelast_fluct acc;
+    // pair list of the pair passes: largest squared displacement this step since its last
+    // refresh, and a forced refresh (after a neighbour-list rebuild)
+    double sub_d2;
+    int sub_force, pad4;
 };
 
 struct TablesView {
@@ -131,6 +135,13 @@ struct AtomsView {
     int *max_count; // [2]: largest neighbour count, largest cell count of the last build
     mdelast_sample *ring; // [n_rep][ring_cap] records of sampled steps (or null)
     int ring_cap, pad_ring;
+    // The list the pair passes read: the neighbour list itself, or its pairs within
+    // sub_r2 (squared radius, cm^2) kept since the coordinates crd_ref; refreshed once some
+    // atom has moved by more than half the radius margin (sub_half2 = that half, squared).
+    int *pnbr, *pn_up, *pn_dn;
+    int pmaxn, pad_p;
+    double4 *crd_ref;     // null: the pair passes read the neighbour list
+    double sub_r2, sub_half2;
 };
 
 // md_driver.hpp:48-50: round half away from zero through a truncating int conversion

@@ -145,6 +145,16 @@ struct mdelast_driver_s {
             launch_force(obs, kick, tpa_f, grid_f, s, A, T);
     }
     int *d_nbr = nullptr, *d_nup = nullptr, *d_ndn = nullptr;
+    // pair list of the pair passes (see AtomsView::pnbr); pair_factor 0: the neighbour list
+    int *d_pnbr = nullptr, *d_pnup = nullptr, *d_pndn = nullptr;
+    double4 *d_crd_ref = nullptr;
+    double pair_factor = 0., rcut0 = 0.;
+    int set_pair_list(double factor);
+    void point_pair_list();
+    void refresh_pair_list(cudaStream_t s) {
+        if (A.crd_ref)
+            k_sublist<<<n_pad / 8, 256, 0, s>>>(A);
+    }
     double *d_pd = nullptr, *d_pf = nullptr, *d_red = nullptr;
     // closing scalar work: fold the block sums, then the per-replica kernel
     void post(int mode, int obs, cudaStream_t s) {
@@ -225,6 +235,10 @@ mdelast_driver_s::~mdelast_driver_s() {
     dfree(d_nbr);
     dfree(d_nup);
     dfree(d_ndn);
+    dfree(d_pnbr);
+    dfree(d_pnup);
+    dfree(d_pndn);
+    dfree(d_crd_ref);
     dfree(d_pd);
     dfree(d_pf);
     dfree(d_red);
@@ -254,7 +268,66 @@ int mdelast_driver_s::alloc_list(int maxn) {
         return rc;
     A.nbr = d_nbr;
     A.maxn = maxn;
+    if (pair_factor > 0.) {
+        dfree(d_pnbr);
+        if (int rc = dalloc(&d_pnbr, static_cast<size_t>(maxn) * n_pad))
+            return rc;
+    }
+    point_pair_list();
     drop_graphs();
+    return MDELAST_OK;
+}
+
+void mdelast_driver_s::point_pair_list() {
+    if (pair_factor > 0.) {
+        A.pnbr = d_pnbr;
+        A.pn_up = d_pnup;
+        A.pn_dn = d_pndn;
+        A.crd_ref = d_crd_ref;
+        double const rs = pair_factor * rcut0, half = 0.5 * (pair_factor - 1.) * rcut0;
+        A.sub_r2 = rs * rs;
+        A.sub_half2 = half * half;
+    } else {
+        A.pnbr = A.nbr;
+        A.pn_up = A.n_up;
+        A.pn_dn = A.n_dn;
+        A.crd_ref = nullptr;
+        A.sub_r2 = A.sub_half2 = 0.;
+    }
+    A.pmaxn = A.maxn;
+}
+
+// The pair passes read the neighbour list's pairs within factor * r_cut, refreshed when
+// needed (factor 0: the neighbour list itself). Rebuilds the rows now.
+int mdelast_driver_s::set_pair_list(double factor) {
+    if (factor != 0. && !(factor > 1.))
+        return fail(MDELAST_ERR_ARGUMENT, "pair-list radius factor must be 0 or > 1");
+    if (!neighbors || factor >= r_skin)
+        factor = 0.; // without a neighbour list, or no tighter than it: nothing to gain
+    CK(cudaStreamSynchronize(stream));
+    drop_graphs();
+    dfree(d_pnbr);
+    dfree(d_pnup);
+    dfree(d_pndn);
+    dfree(d_crd_ref);
+    pair_factor = factor;
+    if (factor > 0.) {
+        if (int rc = dalloc(&d_pnbr, static_cast<size_t>(A.maxn) * n_pad))
+            return rc;
+        if (int rc = dalloc(&d_pnup, static_cast<size_t>(n_pad)))
+            return rc;
+        if (int rc = dalloc(&d_pndn, static_cast<size_t>(n_pad)))
+            return rc;
+        if (int rc = dalloc(&d_crd_ref, static_cast<size_t>(n_pad)))
+            return rc;
+    }
+    point_pair_list();
+    if (A.crd_ref) {
+        k_sub_invalidate<<<1, 128, 0, stream>>>(A);
+        refresh_pair_list(stream);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(stream));
+    }
     return MDELAST_OK;
 }
 
@@ -445,6 +518,8 @@ int mdelast_driver_s::enqueue_rebuild() {
         k_cell_sort<<<A.n_cells, 128, sizeof(int) * A.cell_cap, stream>>>(A);
     }
     k_nbr_build<<<n_pad / 8, 256, 0, stream>>>(A); // one warp per atom slot
+    if (A.crd_ref)
+        k_sub_invalidate<<<1, 128, 0, stream>>>(A);
     CK(cudaGetLastError());
     return MDELAST_OK;
 }
@@ -488,6 +563,7 @@ int mdelast_driver_s::enqueue_step(int obs, int rebuild) {
     if (!neighbors)
         if (int rc = enqueue_rebuild())
             return rc;
+    refresh_pair_list(stream);
     pass_density(obs != 0, stream);
     pass_force(obs != 0, true, stream);
     post(POST_STEP, obs, stream);
@@ -994,6 +1070,13 @@ static int create_system(const mdelast_driver_config *cfgs, int n_rep, mdelast_d
     TRY(d->build_list_checked());
     if (d->A.posf)
         k_posf<<<np / kBlock, kBlock, 0, d->stream>>>(d->A);
+    {
+        double f = 1.06; // pairs within 1.06 r_cut; MDELAST_PAIR_LIST=0 reads the full list
+        if (char const *e = std::getenv("MDELAST_PAIR_LIST"))
+            f = std::atof(e);
+        d->rcut0 = rcut;
+        TRY(d->set_pair_list(f));
+    }
     d->pass_density(true, d->stream);
     d->pass_force(true, false, d->stream);
     d->post(POST_INIT, 1, d->stream);
@@ -1072,7 +1155,7 @@ int mdelast_driver_kernel_times(mdelast_driver *d, int32_t n_steps, double *ms_o
     CK(cudaSetDevice(d->device));
     if (int rc = d->wait_step())
         return rc;
-    std::vector<cudaEvent_t> ev(7);
+    std::vector<cudaEvent_t> ev(8);
     for (auto &e : ev)
         CK(cudaEventCreate(&e));
     double acc[MDELAST_N_KERNEL_TIMES] = {0, 0, 0, 0, 0, 0};
@@ -1088,6 +1171,8 @@ int mdelast_driver_kernel_times(mdelast_driver *d, int32_t n_steps, double *ms_o
         cudaEventRecord(ev[2], s);
         k_kick_drift<<<grid, kBlock, 0, s>>>(d->A, d->T);
         cudaEventRecord(ev[3], s);
+        d->refresh_pair_list(s);
+        cudaEventRecord(ev[7], s);
         d->pass_density(true, s);
         cudaEventRecord(ev[4], s);
         d->pass_force(true, true, s);
@@ -1099,10 +1184,17 @@ int mdelast_driver_kernel_times(mdelast_driver *d, int32_t n_steps, double *ms_o
             rc = fail(MDELAST_ERR_CUDA, "kernel timing: %s", cudaGetErrorString(e));
             break;
         }
-        float t[6];
+        // pre, kick+drift, density, force, closing scalar work, list build + pair-list
+        // refresh
+        float t[6], u = 0.f;
+        cudaEventElapsedTime(&t[0], ev[1], ev[2]);
+        cudaEventElapsedTime(&t[1], ev[2], ev[3]);
+        cudaEventElapsedTime(&t[2], ev[7], ev[4]);
+        cudaEventElapsedTime(&t[3], ev[4], ev[5]);
+        cudaEventElapsedTime(&t[4], ev[5], ev[6]);
         cudaEventElapsedTime(&t[5], ev[0], ev[1]);
-        for (int k = 0; k < 5; ++k)
-            cudaEventElapsedTime(&t[k], ev[k + 1], ev[k + 2]);
+        cudaEventElapsedTime(&u, ev[3], ev[7]);
+        t[5] += u;
         for (int k = 0; k < 6; ++k)
             acc[k] += t[k];
         ++d->host_cycle;
@@ -1426,6 +1518,16 @@ int mdelast_driver_set_launch(mdelast_driver *d, int32_t tpa_density, int32_t tp
         return rc;
     double md = 0., mf = 0.;
     return d->time_passes(1, 1, &md, &mf);
+}
+
+int mdelast_driver_set_pair_list(mdelast_driver *d, double factor) {
+    clear_error();
+    if (!d)
+        return fail(MDELAST_ERR_ARGUMENT, "null driver");
+    CK(cudaSetDevice(d->device));
+    if (int rc = d->wait_step())
+        return rc;
+    return d->set_pair_list(factor);
 }
 
 int mdelast_driver_set_sample_ring(mdelast_driver *d, int32_t capacity) {

@@ -29,6 +29,8 @@ __global__ void k_pre(AtomsView A);
 __global__ void k_reduce(AtomsView A);
 __global__ void k_post(AtomsView A, int mode, int obs);
 __global__ void k_samples_reset(AtomsView A, int what);
+__global__ void k_sublist(AtomsView A);
+__global__ void k_sub_invalidate(AtomsView A);
 __global__ void k_readout(AtomsView A, TablesView T, int r, int field, double *out,
                           const double *pos0, int stepped);
 __global__ void k_half_list_counts(AtomsView A, int r, int *counts);

@@ -549,6 +549,7 @@ class MDDriver {
     void set_launch(int td, int tf, int bd, int bf) {
         check(mdelast_driver_set_launch(d_, td, tf, bd, bf));
     }
+    void set_pair_list(double f) { check(mdelast_driver_set_pair_list(d_, f)); }
     py::dict drain_samples() { return drain_dict(d_, -1); }
     void fluctuation_start() { check(mdelast_driver_fluct_start(d_)); }
     mdelast_fluct fluct() {
@@ -763,6 +764,7 @@ class BatchedMDDriver {
     void set_launch(int td, int tf, int bd, int bf) {
         check(mdelast_driver_set_launch(d_, td, tf, bd, bf));
     }
+    void set_pair_list(double f) { check(mdelast_driver_set_pair_list(d_, f)); }
     // thermostat (which = 0) or barostat (1) chain of replica r: (q, p_eta, eta)
     py::tuple chain(int r, int which) {
         double q[16], p[16], e[16];
@@ -945,6 +947,8 @@ PYBIND11_MODULE(md_driver_module, m) {
              "time the pair passes over their launch shapes and keep the fastest")
         .def("set_launch", &MDDriver::set_launch, py::arg("tpa_density"), py::arg("tpa_force"),
              py::arg("blocks_density"), py::arg("blocks_force"))
+        .def("set_pair_list", &MDDriver::set_pair_list, py::arg("factor"),
+             "pair passes walk the list's pairs within factor * r_cut (0: the full list)")
         .def("set_sample_ring", &MDDriver::set_sample_ring, py::arg("capacity"),
              "room for this many sampled steps between drains (0: no ring)")
         .def("drain_samples", &MDDriver::drain_samples,
@@ -1001,6 +1005,7 @@ PYBIND11_MODULE(md_driver_module, m) {
         .def("autotune", &BatchedMDDriver::autotune, py::arg("n_repeat") = 3)
         .def("set_launch", &BatchedMDDriver::set_launch, py::arg("tpa_density"),
              py::arg("tpa_force"), py::arg("blocks_density"), py::arg("blocks_force"))
+        .def("set_pair_list", &BatchedMDDriver::set_pair_list, py::arg("factor"))
         .def("set_sample_ring", &BatchedMDDriver::set_sample_ring, py::arg("capacity"))
         .def("drain_samples", &BatchedMDDriver::drain_samples, py::arg("replica"))
         .def("chain", &BatchedMDDriver::chain, py::arg("replica"), py::arg("which") = 0)

@@ -164,13 +164,13 @@ __global__ void __launch_bounds__(kBlock) k_density_mx(AtomsView A, TablesView T
         if (valid) {
             float4 const pi = A.posf[i];
             ti = static_cast<int>(pi.w);
-            int const nu = A.n_up[i], ntot = nu + A.n_dn[i];
-            int const *row = A.nbr + static_cast<size_t>(i) * A.maxn;
-            float4 pn = A.posf[sub < ntot ? row[list_slot(sub, nu, A.maxn)] : i];
+            int const nu = A.pn_up[i], ntot = nu + A.pn_dn[i];
+            int const *row = A.pnbr + static_cast<size_t>(i) * A.pmaxn;
+            float4 pn = A.posf[sub < ntot ? row[list_slot(sub, nu, A.pmaxn)] : i];
             for (int kk = sub; kk < ntot; kk += TPA) {
                 float4 const pj = pn;
                 if (kk + TPA < ntot)
-                    pn = A.posf[row[list_slot(kk + TPA, nu, A.maxn)]];
+                    pn = A.posf[row[list_slot(kk + TPA, nu, A.pmaxn)]];
                 float dx, dy, dz;
                 float const r2 = min_image_f(pi, pj, L, iL, dx, dy, dz);
                 if (r2 > T.fr_cut_sq)
@@ -298,7 +298,7 @@ __device__ __forceinline__ void force_row_mx(AtomsView const &A, TablesView cons
                                              PairSums<OBS> &ps, bool &warn_rmin) {
     if (sub >= n)
         return;
-    auto slot = [&](int k) { return UPPER ? k : A.maxn - 1 - k; };
+    auto slot = [&](int k) { return UPPER ? k : A.pmaxn - 1 - k; };
     int jn = row[slot(sub)];
     float4 pn = A.posf[jn];
     float2 fn = A.dF2f[jn];
@@ -424,8 +424,8 @@ __global__ void __launch_bounds__(kBlock) k_force_mx(AtomsView A, TablesView T) 
             float2 const dFi2 = T.has_eam ? A.dF2f[i] : make_float2(0.f, 0.f);
             in.dFi = dFi2.x;
             in.d2Fi = OBS ? dFi2.y : 0.f;
-            int const nu = A.n_up[i], nd = A.n_dn[i];
-            int const *row = A.nbr + static_cast<size_t>(i) * A.maxn;
+            int const nu = A.pn_up[i], nd = A.pn_dn[i];
+            int const *row = A.pnbr + static_cast<size_t>(i) * A.pmaxn;
             bool warn_rmin = false;
             PairSums<OBS> ps;
             force_row_mx<OBS, true, TPA, IP>(A, T, in, row, nu, sub, fx, fy, fz, epot, ps,

@@ -269,6 +269,7 @@ __global__ void k_pre(AtomsView A) {
     int const ens = R->ensemble;
     double const dt = R->dt;
     if (threadIdx.x == 0) {
+        R->sub_d2 = 0.; // k_kick_drift takes this step's largest displacement
         double ekin = R->obs.ekin_tot;
         double S = 1.;
         if (ens == MDELAST_NVT || ens == MDELAST_NPT) {
@@ -595,6 +596,7 @@ __global__ void k_post(AtomsView A, int mode, int obs) {
     o.sample_observables = obs;
     if (mode == POST_STEP && obs)
         record_sample(A, static_cast<int>(blockIdx.x), R, V);
+    R->sub_force = 0; // a forced pair-list refresh has run by now
 }
 
 } // namespace mdelast
