@@ -91,8 +91,108 @@ __device__ __forceinline__ void nb_batch(AtomsView const &A, int i, int j, bool 
     nd += cd;
 }
 
-// One warp per atom slot; the lanes test 32 candidates at a time.
-__global__ void k_nbr_build(AtomsView A) {
+// Cell-list replicas: one block per cell. The partners of the cell's atoms all lie in its
+// 27 stencil cells, so their records are staged in shared memory once per cell (in chunks
+// of kStage, in the stencil order dz, dy, dx and member order of the per-atom search below)
+// and each warp tests its atoms against the staged records: the same candidates in the same
+// order as the per-atom search, so the same list, without re-gathering every candidate
+// from global memory for each atom of the cell.
+constexpr int kStage = 512;
+
+__global__ void __launch_bounds__(128) k_nbr_cells(AtomsView A) {
+    extern __shared__ unsigned char s_raw[];
+    double4 *s_c = reinterpret_cast<double4 *>(s_raw);
+    int *s_j = reinterpret_cast<int *>(s_c + kStage);
+    int *s_cnt = s_j + kStage;    // [4][cell_cap]: nu, nd, total, full of the cell's atoms
+    __shared__ int s_cell[27], s_off[28];
+    int const cell = blockIdx.x;
+    int const r = A.cell_rep[cell];
+    Replica const &R = A.rep[r];
+    int const loc = cell - R.cell_begin;
+    int const cx0 = loc % R.nc[0], cy0 = (loc / R.nc[0]) % R.nc[1],
+              cz0 = loc / (R.nc[0] * R.nc[1]);
+    int const cap = A.cell_cap;
+    int const n_me = min(A.cell_count[cell], cap);
+    int const *me = A.cell_atoms + static_cast<size_t>(cell) * cap;
+    int *c_nu = s_cnt, *c_nd = s_cnt + cap, *c_tot = s_cnt + 2 * cap, *c_full = s_cnt + 3 * cap;
+    for (int a = threadIdx.x; a < n_me; a += blockDim.x)
+        c_nu[a] = c_nd[a] = c_tot[a] = c_full[a] = 0;
+    if (threadIdx.x == 0) {
+        int q = 0, off = 0;
+        for (int dz = -1; dz <= 1; ++dz) {
+            int const cz = (cz0 + dz + R.nc[2]) % R.nc[2];
+            for (int dy = -1; dy <= 1; ++dy) {
+                int const cy = (cy0 + dy + R.nc[1]) % R.nc[1];
+                for (int dx = -1; dx <= 1; ++dx, ++q) {
+                    int const cx = (cx0 + dx + R.nc[0]) % R.nc[0];
+                    int const c = R.cell_begin + (cz * R.nc[1] + cy) * R.nc[0] + cx;
+                    s_cell[q] = c;
+                    s_off[q] = off;
+                    off += min(A.cell_count[c], cap);
+                }
+            }
+        }
+        s_off[27] = off;
+    }
+    __syncthreads();
+    int const M = s_off[27];
+    unsigned const lane = threadIdx.x & 31u;
+    int const warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    double const hx = R.h[0], hy = R.h[1], hz = R.h[2];
+    double const rl2 = A.r_list_sq;
+    for (int c0 = 0; c0 < M; c0 += kStage) {
+        int const len = min(kStage, M - c0);
+        for (int t = threadIdx.x; t < len; t += blockDim.x) {
+            int const g = c0 + t;
+            int q = 0;
+            while (s_off[q + 1] <= g)
+                ++q;
+            int const j = A.cell_atoms[static_cast<size_t>(s_cell[q]) * cap + (g - s_off[q])];
+            s_j[t] = j;
+            s_c[t] = A.crd[j];
+        }
+        __syncthreads();
+        for (int a = warp; a < n_me; a += nwarp) {
+            int const i = me[a];
+            double4 const ci = A.crd[i];
+            int nu = c_nu[a], nd = c_nd[a], total = c_tot[a];
+            bool full = c_full[a] != 0;
+            for (int base = 0; base < len; base += 32) {
+                int const k = base + static_cast<int>(lane);
+                int const j = k < len ? s_j[k] : -1;
+                bool hit = false;
+                if (k < len && j != i) {
+                    double px, py, pz;
+                    hit = min_image_r2(ci, s_c[k], hx, hy, hz, px, py, pz) <= rl2;
+                }
+                nb_batch(A, i, j, hit, lane, nu, nd, total, full);
+            }
+            if (lane == 0) {
+                c_nu[a] = nu;
+                c_nd[a] = nd;
+                c_tot[a] = total;
+                c_full[a] = full ? 1 : 0;
+            }
+        }
+        __syncthreads();
+    }
+    for (int a = threadIdx.x; a < n_me; a += blockDim.x) {
+        int const i = me[a];
+        A.n_up[i] = c_nu[a];
+        A.n_dn[i] = c_nd[a];
+        if (c_tot[a] > A.maxn)
+            status_or(&A.rep[r], MDELAST_ERR_LIST_OVERFLOW);
+        atomicMax(&A.max_count[0], c_tot[a]);
+    }
+}
+
+size_t nbr_cells_smem(int cell_cap) {
+    return (sizeof(double4) + sizeof(int)) * kStage + 4 * sizeof(int) * cell_cap;
+}
+
+// One warp per atom slot; the lanes test 32 candidates at a time. Atoms of cell-list
+// replicas are left to k_nbr_cells when cells_done.
+__global__ void k_nbr_build(AtomsView A, int cells_done) {
     unsigned const lane = threadIdx.x & 31u;
     int const i = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (i >= A.n_pad)
@@ -106,6 +206,8 @@ __global__ void k_nbr_build(AtomsView A) {
         return;
     }
     Replica const &R = A.rep[r];
+    if (cells_done && R.nc[0] != 0)
+        return;
     double4 const ci = A.crd[i];
     double const hx = R.h[0], hy = R.h[1], hz = R.h[2];
     double const rl2 = A.r_list_sq;

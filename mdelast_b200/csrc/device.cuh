@@ -130,6 +130,7 @@ struct AtomsView {
     const int *dblk_rep, *fblk_rep; // replica of each block of the density / force pass
     // cell list (list builds)
     int *cell_count, *cell_atoms;
+    const int *cell_rep; // replica of each cell
     int cell_cap, n_cells;
     double r_list_sq;
     int *max_count; // [2]: largest neighbour count, largest cell count of the last build

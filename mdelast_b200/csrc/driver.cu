@@ -162,6 +162,8 @@ struct mdelast_driver_s {
         k_post<<<n_rep, 256, 0, s>>>(A, mode, obs);
     }
     int *d_cell_count = nullptr, *d_cell_atoms = nullptr, *d_max_count = nullptr;
+    int *d_cell_rep = nullptr;
+    std::vector<int> cell_rep_host; // replica of each cell, as uploaded
     double *d_rb = nullptr, *d_Ft = nullptr;
     double *d_pos0 = nullptr, *d_out = nullptr;
     int *d_tmp_i = nullptr;
@@ -244,6 +246,7 @@ mdelast_driver_s::~mdelast_driver_s() {
     dfree(d_red);
     dfree(d_cell_count);
     dfree(d_cell_atoms);
+    dfree(d_cell_rep);
     dfree(d_max_count);
     dfree(d_rb);
     dfree(d_Ft);
@@ -334,8 +337,13 @@ int mdelast_driver_s::set_pair_list(double factor) {
 int mdelast_driver_s::alloc_cells(int n_cells, int cell_cap) {
     dfree(d_cell_count);
     dfree(d_cell_atoms);
+    dfree(d_cell_rep);
+    cell_rep_host.clear();
     if (int rc = dalloc(&d_cell_count, static_cast<size_t>(std::max(n_cells, 1))))
         return rc;
+    if (int rc = dalloc(&d_cell_rep, static_cast<size_t>(std::max(n_cells, 1))))
+        return rc;
+    A.cell_rep = d_cell_rep;
     if (int rc = dalloc(&d_cell_atoms, static_cast<size_t>(std::max(n_cells, 1)) * cell_cap))
         return rc;
     A.cell_count = d_cell_count;
@@ -494,6 +502,18 @@ int mdelast_driver_s::configure_cells(std::vector<double> const &boxes) {
     if (!d_cell_count || n_cells > cells_alloc || cap > A.cell_cap)
         if (int rc = alloc_cells(std::max(n_cells, cells_alloc), cap))
             return rc;
+    std::vector<int> crep;
+    for (int q = 0; q < n_rep; ++q) {
+        Replica const &x = R[static_cast<size_t>(q)];
+        if (x.nc[0] > 0)
+            crep.insert(crep.end(), static_cast<size_t>(x.nc[0]) * x.nc[1] * x.nc[2], q);
+    }
+    if (crep != cell_rep_host) {
+        if (!crep.empty())
+            CK(cudaMemcpy(d_cell_rep, crep.data(), sizeof(int) * crep.size(),
+                          cudaMemcpyHostToDevice));
+        cell_rep_host = crep;
+    }
     if (changed || all_pairs != all_brute || A.n_cells != n_cells)
         drop_graphs(); // the launch shape of the cell kernels is part of the graphs
     all_pairs = all_brute;
@@ -517,7 +537,17 @@ int mdelast_driver_s::enqueue_rebuild() {
         k_cell_bin<<<grid, kBlock, 0, stream>>>(A);
         k_cell_sort<<<A.n_cells, 128, sizeof(int) * A.cell_cap, stream>>>(A);
     }
-    k_nbr_build<<<n_pad / 8, 256, 0, stream>>>(A); // one warp per atom slot
+    int cells_done = 0;
+    if (!all_pairs && A.n_cells > 0) {
+        size_t const smem = nbr_cells_smem(A.cell_cap);
+        if (smem > 48 * 1024)
+            CK(cudaFuncSetAttribute(k_nbr_cells, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(smem)));
+        k_nbr_cells<<<A.n_cells, 128, smem, stream>>>(A);
+        cells_done = 1;
+    }
+    // all-pairs replicas and padding slots: one warp per atom slot
+    k_nbr_build<<<n_pad / 8, 256, 0, stream>>>(A, cells_done);
     if (A.crd_ref)
         k_sub_invalidate<<<1, 128, 0, stream>>>(A);
     CK(cudaGetLastError());

@@ -10,7 +10,9 @@ enum PostMode : int { POST_INIT = 0, POST_STEP = 1 };
 
 __global__ void k_cell_bin(AtomsView A);
 __global__ void k_cell_sort(AtomsView A);
-__global__ void k_nbr_build(AtomsView A);
+__global__ void k_nbr_build(AtomsView A, int cells_done);
+__global__ void k_nbr_cells(AtomsView A);
+size_t nbr_cells_smem(int cell_cap); // dynamic shared memory of k_nbr_cells
 // launchers of the templated pair kernels (defined beside them); tpa = lanes per atom,
 // one of 1, 4, 8, 16 (valid_tpa)
 bool valid_tpa(int tpa);
