@@ -19,7 +19,8 @@ final positions and velocities read back; wall-clock time of all of it.
 time_to_cij (rank 0, --no-cij skips it): wall time to C11/C12/C44 within 2 % of the FP64
 plain protocol's result, the plain protocol (one FP64 cell, NPT then NVT as the reference's
 sample case, 120k steps) against 4 mixed-precision replicas started in the box the trained
-warm-start network proposes (see time_to_cij).
+warm-start network proposes (see time_to_cij). --cij-nialco adds the same comparison for
+the 108,000-atom Ni-Al-Co cell and the ternary network (see time_to_cij_nialco).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--replicas R] [--precision fp64|mixed]
@@ -227,6 +228,9 @@ def run_ours(args, rank, world, local_rank):
     cij = None
     if rank == 0 and not args.no_cij:
         cij = time_to_cij(m, t, cpu)
+    cij_nialco = None
+    if rank == 0 and args.cij_nialco:
+        cij_nialco = time_to_cij_nialco(m)
     others = None if args.no_configs else other_configs(m, t, local_rank)
     n_rebuilds = (args.steps + REBUILD - 1) // REBUILD
     launches = args.steps * 6 + n_rebuilds * 3
@@ -247,6 +251,7 @@ def run_ours(args, rank, world, local_rank):
                    "launch": tune},
         "plain_fp64_single_cell": plain,
         "time_to_cij": cij,
+        "time_to_cij_nialco_108000": cij_nialco,
         "other_configs": others,
         "roofline": roof,
         "cpu_baseline": cpu,
@@ -370,6 +375,67 @@ def time_to_cij(m, t, cpu):
     return out
 
 
+NIALCO_NSIDE = 30  # 108,000 atoms
+NIALCO_SEED = 5    # composition: RandomState(5).dirichlet((2, 2, 2))
+
+
+def time_to_cij_nialco(m):
+    """Wall time to C11/C12/C44 of a random Ni-Al-Co FCC 30^3 cell (108,000 atoms) at
+    300 K, composition one Dirichlet(2, 2, 2) draw, bundled Mishin 2013 potential.
+
+    plain: the same FP64 protocol as the Cu-Zn comparison, started at the linear (Vegard)
+    lattice constant; its final C_ij is the target. warm start: the ternary network
+    proposes the lattice constant and the bulk modulus; one cell in the proposed box, mixed
+    precision, 500 NVT thermalisation steps, production sampled every 5th step; its first
+    500 production steps are the judge's window (0.2 GPa), with at most one box correction
+    from the window pressure and the proposed bulk modulus before the plain protocol takes
+    over. Times as in time_to_cij."""
+    import numpy as np
+
+    from mdelast_b200.potentials import find_potential, read_setfl
+    from mdelast_b200.protocol import Stages, run_protocol, run_warm_start, time_to_within
+    from mdelast_b200.systems import fcc_alloy_cell
+    from mdelast_b200.warmstart import (NIALCO_MODEL, NIALCO_POTENTIAL, WarmStart, judge,
+                                        nialco_guess_a)
+    t = read_setfl(find_potential(NIALCO_POTENTIAL))
+    x = np.random.RandomState(NIALCO_SEED).dirichlet((2.0, 2.0, 2.0))
+    a_lin = nialco_guess_a(x, T_K)
+    kw = dict(T=T_K, placement_seed=11)
+    plain = run_protocol(m, t, [fcc_alloy_cell(t, NIALCO_NSIDE, x, a_ang=a_lin, ensemble=2,
+                                               velocity_seed=0, **kw)],
+                         precision="fp64", stages=Stages(**PLAIN_STAGES), nvt_seeds=[1])
+    target = plain.C
+    t0 = time.perf_counter()
+    ws = WarmStart.load(NIALCO_MODEL)
+    prop = ws.propose(x, T_K)
+    cells = [fcc_alloy_cell(t, NIALCO_NSIDE, x, a_ang=float(prop["a"][0]), ensemble=1,
+                            velocity_seed=200, **kw)]
+    setup = time.perf_counter() - t0
+    warm = run_warm_start(m, t, cells, precision="mixed", stages=Stages(**WARM_STAGES),
+                          judge=judge, check_steps=500, bulk_GPa=[float(prop["B"][0])])
+    t_warm = time_to_within(warm, target, CIJ_TOL)
+    t_warm = None if t_warm is None else setup + t_warm
+    t_plain_self = time_to_within(plain, target, CIJ_TOL)
+    a_npt = a_lin * plain.V_V0[0] ** (1.0 / 3.0)
+    return {
+        "unit": "s", "cell": f"nialco_fcc{NIALCO_NSIDE}_{4 * NIALCO_NSIDE**3}_npt300",
+        "fractions_ni_al_co": x.tolist(), "tolerance": CIJ_TOL,
+        "plain_fp64": {"wall_s": plain.wall_s, "C_GPa": plain.C, "steps": 120000,
+                       "own_time_to_within_s": t_plain_self, "a_npt": a_npt,
+                       "a_linear_guess": a_lin},
+        "warm_start_mixed": {"time_to_within_s": t_warm, "wall_s": setup + warm.wall_s,
+                             "C_GPa": warm.C,
+                             "rel_err_vs_plain": {k: warm.C[k] / target[k] - 1 for k in target},
+                             "proposal": {k: float(v[0]) for k, v in prop.items()},
+                             "a_rel_err_vs_npt": float(prop["a"][0]) / a_npt - 1,
+                             "accepted": warm.accepted_start, "corrections": warm.corrections,
+                             "window_pressure_GPa": warm.npt_pressure_GPa},
+        "speedup_vs_plain_protocol": (plain.wall_s / t_warm) if t_warm else None,
+        "speedup_vs_plain_time_to_within": (t_plain_self / t_warm)
+        if (t_warm and t_plain_self) else None,
+    }
+
+
 def half_list_nbar(m, t, cell):
     """Half-list entries per atom of the reference's list at this cell (point[N]/N)."""
     from mdelast_b200.systems import make_driver
@@ -475,6 +541,9 @@ def main():
                     help="skip the other workloads (64 uneven replicas, L1_2 32k cell)")
     ap.add_argument("--no-cij", action="store_true",
                     help="skip the time-to-C_ij comparison (plain FP64 protocol vs warm start)")
+    ap.add_argument("--cij-nialco", action="store_true",
+                    help="also time C_ij of the 108,000-atom Ni-Al-Co cell: plain FP64 "
+                         "protocol vs the ternary warm start (adds about 3 minutes)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -254,6 +254,10 @@ int mdelast_batch_get_chain(mdelast_driver *d, int32_t replica, int32_t which, d
                             double *p_eta, double *eta, int32_t *nchain);
 int mdelast_batch_get_neighbors(mdelast_driver *d, int32_t replica, int32_t *point,
                                 int32_t *neighbors, int64_t cap, int64_t *n_entries);
+/* Status word of every replica (MDELAST_FATAL_* / MDELAST_ERR_* / MDELAST_WARN_* bits)
+ * after the queued steps, into status[n_replicas]. Unlike the readouts above it succeeds
+ * after a FATAL bit has stopped the batch, so a caller can tell which replica raised it. */
+int mdelast_batch_get_status(mdelast_driver *d, uint32_t *status);
 
 /* Pair correlation (md_driver.cpp:732-862): mode 0 calculate_pair_correlation,
  * 1 calculate_pair_correlations, 2 calculate_partial_pair_correlation. gr has n_rg

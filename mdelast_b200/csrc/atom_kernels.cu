@@ -11,8 +11,33 @@ namespace mdelast {
 
 // ------------------------------------------------------------------------------------
 // neighbour list (md_driver.cpp:279-298): every pair with the reference's min-image
-// |p|^2 <= (rcut r_skin)^2, found through a cell list with cells no smaller than the list
-// radius (or all pairs when a replica has fewer than 3 cells along an edge).
+// |p|^2 <= (rcut r_skin)^2, found through a cell list (or all pairs when a replica has
+// fewer than 3 cells along an edge). The cell grid is fixed when a run starts; a barostat
+// may shrink the box below it between builds, so each build takes, along every edge, the
+// reach k (cells either side) with k * h / nc >= the list radius in the current box.
+
+// reach along one edge of h with nc cells (1 while the cells are no narrower than the
+// list radius, as they start)
+__device__ __forceinline__ int cell_reach(double h, int nc, double rl2) {
+    double const w = h / nc;
+    int k = 1;
+    while (k < nc && (k * w) * (k * w) < rl2)
+        ++k;
+    return k;
+}
+
+// the distinct cells of one edge the stencil spans from cell idx: count, and the first
+// (all nc cells from 0 once 2k + 1 exceeds the edge)
+__device__ __forceinline__ void cell_span(int idx, int nc, int k, int &first, int &count) {
+    bool const fits = 2 * k + 1 <= nc;
+    count = fits ? 2 * k + 1 : nc;
+    first = fits ? idx - k : 0;
+}
+
+__device__ __forceinline__ bool narrow_cells(Replica const &R, double rl2) {
+    return cell_reach(R.h[0], R.nc[0], rl2) > 1 || cell_reach(R.h[1], R.nc[1], rl2) > 1 ||
+           cell_reach(R.h[2], R.nc[2], rl2) > 1;
+}
 
 __global__ void k_cell_bin(AtomsView A) {
     int const i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -96,7 +121,8 @@ __device__ __forceinline__ void nb_batch(AtomsView const &A, int i, int j, bool 
 // of kStage, in the stencil order dz, dy, dx and member order of the per-atom search below)
 // and each warp tests its atoms against the staged records: the same candidates in the same
 // order as the per-atom search, so the same list, without re-gathering every candidate
-// from global memory for each atom of the cell.
+// from global memory for each atom of the cell. Replicas whose box has shrunk below the
+// cell grid (reach > 1) are left to k_nbr_build.
 constexpr int kStage = 512;
 
 __global__ void __launch_bounds__(128) k_nbr_cells(AtomsView A) {
@@ -108,6 +134,8 @@ __global__ void __launch_bounds__(128) k_nbr_cells(AtomsView A) {
     int const cell = blockIdx.x;
     int const r = A.cell_rep[cell];
     Replica const &R = A.rep[r];
+    if (narrow_cells(R, A.r_list_sq))
+        return;
     int const loc = cell - R.cell_begin;
     int const cx0 = loc % R.nc[0], cy0 = (loc / R.nc[0]) % R.nc[1],
               cz0 = loc / (R.nc[0] * R.nc[1]);
@@ -191,7 +219,7 @@ size_t nbr_cells_smem(int cell_cap) {
 }
 
 // One warp per atom slot; the lanes test 32 candidates at a time. Atoms of cell-list
-// replicas are left to k_nbr_cells when cells_done.
+// replicas are left to k_nbr_cells when cells_done, unless their cells are narrow.
 __global__ void k_nbr_build(AtomsView A, int cells_done) {
     unsigned const lane = threadIdx.x & 31u;
     int const i = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -206,11 +234,11 @@ __global__ void k_nbr_build(AtomsView A, int cells_done) {
         return;
     }
     Replica const &R = A.rep[r];
-    if (cells_done && R.nc[0] != 0)
+    double const rl2 = A.r_list_sq;
+    if (cells_done && R.nc[0] != 0 && !narrow_cells(R, rl2))
         return;
     double4 const ci = A.crd[i];
     double const hx = R.h[0], hy = R.h[1], hz = R.h[2];
-    double const rl2 = A.r_list_sq;
     int nu = 0, nd = 0, total = 0;
     bool full = false;
     double px, py, pz;
@@ -231,12 +259,16 @@ __global__ void k_nbr_build(AtomsView A, int cells_done) {
             int k = static_cast<int>(floor((w[a] + 0.5) * R.nc[a]));
             idx[a] = k < 0 ? 0 : (k >= R.nc[a] ? R.nc[a] - 1 : k);
         }
-        for (int dz = -1; dz <= 1; ++dz) {
-            int const cz = (idx[2] + dz + R.nc[2]) % R.nc[2];
-            for (int dy = -1; dy <= 1; ++dy) {
-                int const cy = (idx[1] + dy + R.nc[1]) % R.nc[1];
-                for (int dx = -1; dx <= 1; ++dx) {
-                    int const cx = (idx[0] + dx + R.nc[0]) % R.nc[0];
+        int first[3], count[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+            cell_span(idx[a], R.nc[a], cell_reach(R.h[a], R.nc[a], rl2), first[a], count[a]);
+        for (int dz = 0; dz < count[2]; ++dz) {
+            int const cz = (first[2] + dz + R.nc[2]) % R.nc[2];
+            for (int dy = 0; dy < count[1]; ++dy) {
+                int const cy = (first[1] + dy + R.nc[1]) % R.nc[1];
+                for (int dx = 0; dx < count[0]; ++dx) {
+                    int const cx = (first[0] + dx + R.nc[0]) % R.nc[0];
                     int const cell = R.cell_begin + (cz * R.nc[1] + cy) * R.nc[0] + cx;
                     int n = A.cell_count[cell];
                     if (n > A.cell_cap)

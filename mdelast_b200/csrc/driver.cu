@@ -1638,6 +1638,20 @@ int mdelast_batch_get_observables(mdelast_driver *d, int32_t replica, mdelast_ob
     return get_observables_r(d, replica, out);
 }
 
+int mdelast_batch_get_status(mdelast_driver *d, uint32_t *status) {
+    clear_error();
+    if (!d || !status)
+        return fail(MDELAST_ERR_ARGUMENT, "bad argument");
+    CK(cudaSetDevice(d->device));
+    if (!d->obs_valid) {
+        CK(cudaEventSynchronize(d->ev_step));
+        d->obs_valid = true;
+    }
+    for (int r = 0; r < d->n_rep; ++r)
+        status[r] = d->h_obs[r].status;
+    return MDELAST_OK;
+}
+
 int mdelast_batch_get_atoms(mdelast_driver *d, int32_t replica, int32_t field, double *out) {
     return get_atoms_r(d, replica, field, out);
 }

@@ -742,6 +742,11 @@ class BatchedMDDriver {
         check(mdelast_batch_get_observables(d_, r, &o));
         return obs_dict(o);
     }
+    py::array_t<uint32_t> status() {
+        py::array_t<uint32_t> a(static_cast<size_t>(n_replicas()));
+        check(mdelast_batch_get_status(d_, a.mutable_data()));
+        return a;
+    }
     py::array_t<double> atoms(int r, int field) {
         if (r < 0 || r >= n_replicas())
             throw py::index_error("replica index out of range");
@@ -1000,6 +1005,7 @@ PYBIND11_MODULE(md_driver_module, m) {
         .def("calculate_neighbors", &BatchedMDDriver::calculate_neighbors)
         .def_property("sample_observables", &BatchedMDDriver::get_sample, &BatchedMDDriver::set_sample)
         .def("observables", &BatchedMDDriver::observables, py::arg("replica"))
+        .def("status", &BatchedMDDriver::status)
         .def("atoms", &BatchedMDDriver::atoms, py::arg("replica"), py::arg("field"))
         .def("kernel_times", &BatchedMDDriver::kernel_times, py::arg("n_steps") = 10)
         .def("autotune", &BatchedMDDriver::autotune, py::arg("n_repeat") = 3)

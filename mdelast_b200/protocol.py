@@ -57,6 +57,7 @@ class ProtocolResult:
     wall_s: float = 0.0
     wall_npt_s: float = 0.0
     accepted_start: bool = True
+    corrections: int = 0        # box corrections of a warm start before it was accepted
 
 
 def _nvt_cells(tables, cells, positions, coordinates, V_V0, seeds, handoff):
@@ -68,7 +69,7 @@ def _nvt_cells(tables, cells, positions, coordinates, V_V0, seeds, handoff):
     misfit that takes the NVT stage tens of picoseconds to anneal). "box": the snapshot's
     scaled coordinates placed in the mean box. Both draw fresh velocities and chain
     momenta from the seed, as the reference's NVT stage does. "continue": like "box", with
-    the NPT stage's velocities and thermostat momenta carried over."""
+    the NPT stage's velocities, thermostat momenta and thermostat masses carried over."""
     out = []
     for k, (c, v, seed) in enumerate(zip(cells, V_V0, seeds)):
         scale = v ** (1.0 / 3.0)
@@ -80,11 +81,11 @@ def _nvt_cells(tables, cells, positions, coordinates, V_V0, seeds, handoff):
             pos = (u - np.floor(u + 0.5)) * L
         mass = np.array(tables.masses)[c.types]
         st = initial_state(mass, c.T, c.T, 5e-14, 5e-13, random_seed=seed)
-        vel, p_eta = st.velocities, st.thermo_p_eta
+        vel, p_eta, q = st.velocities, st.thermo_p_eta, st.thermo_q
         if handoff == "continue":
-            vel, p_eta = positions[k][1], positions[k][2]
+            vel, p_eta, q = positions[k][1], positions[k][2], c.thermo_q
         out.append(replace(c, positions=pos, velocities=np.asarray(vel), box=L, ensemble=1,
-                           thermo_q=st.thermo_q, thermo_p_eta=np.asarray(p_eta),
+                           thermo_q=np.asarray(q), thermo_p_eta=np.asarray(p_eta),
                            baro_q=st.baro_q, baro_p_eta=st.baro_p_eta, baro_w=st.baro_w,
                            baro_p_eps=st.baro_p_eps, Nf=st.Nf))
     return out
@@ -180,35 +181,63 @@ def time_to_within(result: ProtocolResult, target: dict, tol: float = 0.02):
     return ok_from
 
 
+def _corrected_cells(m, b, cells, p_GPa, bulk_GPa):
+    """The batch's current states in boxes scaled by 1 + p / (3 B) per edge (one Newton
+    step of p(V) = -B ln(V / V_eq)): scaled coordinates, velocities and thermostat
+    momenta carried over."""
+    out = []
+    for r, c in enumerate(cells):
+        L = c.box * (1.0 + p_GPa[r] / (3.0 * bulk_GPa[r]))
+        u = np.asarray(b.atoms(r, m.ATOM_COORDINATES), dtype=float)
+        out.append(replace(c, positions=(u - np.floor(u + 0.5)) * L, box=L,
+                           velocities=np.asarray(b.atoms(r, m.ATOM_VELOCITIES)),
+                           thermo_p_eta=np.asarray(b.chain(r, 0)[1])))
+    return out
+
+
 def run_warm_start(m, tables, cells: list[Cell], precision="mixed",
                    stages: Stages | None = None, judge=None, check_steps=1000,
-                   fallback: Stages | None = None, autotune=True) -> ProtocolResult:
+                   fallback: Stages | None = None, autotune=True, bulk_GPa=None,
+                   max_corrections=1) -> ProtocolResult:
     """The production run started in a proposed equilibrium box (`cells`, NVT, built at
     the proposed lattice constant), with no NPT stage: NVT thermalisation, then production
     whose first `check_steps` steps also serve as the acceptance window. If `judge(p_GPa)`
-    rejects any replica's mean pressure over that window, the proposal is discarded and
-    the plain protocol (run_protocol with `fallback` stages) runs from the same cells."""
+    rejects any replica's mean pressure over that window and the proposal's bulk moduli
+    `bulk_GPa` are given, every box is corrected from its window pressure
+    (_corrected_cells) and thermalisation (half as long) and window rerun, up to
+    `max_corrections` times; a proposal still rejected is discarded and the plain protocol
+    (run_protocol with `fallback` stages) runs from the original cells."""
     st = stages or Stages(npt_therm=0, npt_prod=0, nvt_therm=1000, nvt_prod=2000,
                           sample_stride=5, checkpoint_every=500)
     t0 = time.perf_counter()
-    b = make_batch(m, tables, [replace(c, ensemble=1) for c in cells], r_skin=1.2,
-                   precision=precision)
-    if autotune:
-        b.autotune(2)
-    b.run(st.nvt_therm, st.rebuild_every, st.sample_stride, False)
-    for r in range(b.n_replicas):
-        b.drain_samples(r)
-    b.fluctuation_start()
+    work = [replace(c, ensemble=1) for c in cells]
     n = min(check_steps, st.nvt_prod)
-    b.run(n, st.rebuild_every, st.sample_stride, False)
-    p = [float(np.mean(b.drain_samples(r)["pressure"])) / U.GPa for r in range(b.n_replicas)]
-    if judge is not None and not all(judge(x) for x in p):
+    corrections, therm = 0, st.nvt_therm
+    while True:
+        b = make_batch(m, tables, work, r_skin=1.2, precision=precision)
+        if autotune:
+            b.autotune(2)
+        b.run(therm, st.rebuild_every, st.sample_stride, False)
+        for r in range(b.n_replicas):
+            b.drain_samples(r)
+        b.fluctuation_start()
+        b.run(n, st.rebuild_every, st.sample_stride, False)
+        p = [float(np.mean(b.drain_samples(r)["pressure"])) / U.GPa
+             for r in range(b.n_replicas)]
+        if judge is None or all(judge(x) for x in p):
+            break
+        if bulk_GPa is None or corrections >= max_corrections:
+            del b
+            res = run_protocol(m, tables, cells, precision=precision,
+                               stages=fallback or Stages(), autotune=autotune)
+            res.accepted_start = False
+            res.corrections = corrections
+            res.wall_s = time.perf_counter() - t0
+            return res
+        work = _corrected_cells(m, b, work, p, bulk_GPa)
         del b
-        res = run_protocol(m, tables, cells, precision=precision, stages=fallback or Stages(),
-                           autotune=autotune)
-        res.accepted_start = False
-        res.wall_s = time.perf_counter() - t0
-        return res
+        corrections += 1
+        therm = st.nvt_therm // 2
     b.set_sample_ring(0)
     done, checkpoints, Cr = n, [], []
     while True:
@@ -224,8 +253,10 @@ def run_warm_start(m, tables, cells: list[Cell], precision="mixed",
     wall = time.perf_counter() - t0
     C_rep = [{k: c[k] / U.GPa for k in ("C11", "C12", "C44")} for c in Cr]
     C = {k: float(np.mean([c[k] for c in C_rep])) for k in ("C11", "C12", "C44")}
-    return ProtocolResult(precision=precision, replicas=len(cells),
-                          atoms_per_replica=cells[0].n_atoms, stages=st,
-                          V_V0=[1.0] * len(cells), npt_pressure_GPa=p, C=C, C_replicas=C_rep,
-                          checkpoints=checkpoints, wall_s=wall, wall_npt_s=0.0,
-                          accepted_start=True)
+    res = ProtocolResult(precision=precision, replicas=len(cells),
+                         atoms_per_replica=cells[0].n_atoms, stages=st,
+                         V_V0=[float(np.prod(w.box) / np.prod(c.box)) for w, c in zip(work, cells)],
+                         npt_pressure_GPa=p, C=C, C_replicas=C_rep,
+                         checkpoints=checkpoints, wall_s=wall, wall_npt_s=0.0,
+                         accepted_start=True, corrections=corrections)
+    return res

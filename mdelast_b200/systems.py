@@ -53,9 +53,11 @@ class Cell:
         return len(self.positions)
 
 
-def _state(tables, positions, types, L, T, ensemble, seed, meta):
+def _state(tables, positions, types, L, T, ensemble, seed, meta, mass_T=None):
+    """Velocities at T and chain masses at mass_T (default T: the reference's choice,
+    Q, W proportional to kT)."""
     mass = np.array(tables.masses)[types]
-    st = initial_state(mass, T, T, 5e-14, 5e-13, random_seed=seed)
+    st = initial_state(mass, T, T if mass_T is None else mass_T, 5e-14, 5e-13, random_seed=seed)
     return Cell(positions=positions, velocities=st.velocities, types=np.asarray(types, np.uint32),
                 box=np.asarray(L, dtype=float), T=T, ensemble=ensemble,
                 thermo_q=st.thermo_q, thermo_p_eta=st.thermo_p_eta, baro_q=st.baro_q,
@@ -74,6 +76,25 @@ def cuzn_cell(tables: SetflTables, nside: int, n_zn: int | None = None, x_zn: fl
     types = substitute(n, n_zn, placement_seed, names.index("Cu"), names.index("Zn"))
     return _state(tables, pos, types, [L] * 3, T, ensemble, velocity_seed,
                   {"kind": "cuzn_fcc", "nside": nside, "n_zn": n_zn, "a_ang": a_ang})
+
+
+def fcc_alloy_cell(tables: SetflTables, nside: int, fractions, T: float = 300.0,
+                   a_ang: float = 3.6, ensemble: int = 1, placement_seed: int = 42,
+                   velocity_seed: int = 0, mass_T: float | None = None) -> Cell:
+    """Random substitutional FCC solid solution of the potential's elements (in file order)
+    with the given fractions: round(x_k N) sites of each type (the rest to the last type),
+    placed by RandomState(placement_seed).permutation. mass_T, when given, is the
+    temperature the thermostat and barostat masses are set for (the target stays T)."""
+    pos, L = fcc_lattice(nside, a_ang * U.angstrom)
+    n = len(pos)
+    x = np.asarray(fractions, dtype=float)
+    counts = np.floor(x / x.sum() * n + 0.5).astype(int)
+    counts[-1] = n - counts[:-1].sum()
+    types = np.repeat(np.arange(len(x), dtype=np.uint32), counts)
+    types = types[np.random.RandomState(placement_seed).permutation(n)]
+    return _state(tables, pos, types, [L] * 3, T, ensemble, velocity_seed,
+                  {"kind": "fcc_alloy", "nside": nside, "counts": counts.tolist(),
+                   "a_ang": a_ang}, mass_T=mass_T)
 
 
 def l12_cell(tables: SetflTables, n: int, T: float = 5.0, ensemble: int = 1,

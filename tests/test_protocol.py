@@ -59,3 +59,104 @@ def test_time_to_within_needs_to_stay_inside():
     assert time_to_within(r, target, tol=0.001) == 4.0
     r.checkpoints.append((5, 5.0, 90, 50, 40))
     assert time_to_within(r, target) is None
+
+
+def test_continue_handoff_keeps_the_npt_thermostat_masses():
+    c = _cell()
+    c.thermo_q = np.full(10, 7.0)  # masses of the NPT stage (e.g. set for a floor temperature)
+    snap = [(np.zeros((8, 3)), np.ones((8, 3)), [0.25] * 10)]
+    (nv,) = _nvt_cells(_Tables, [c], snap, [np.zeros((8, 3))], [1.0], [7], "continue")
+    assert np.array_equal(nv.thermo_q, c.thermo_q)
+
+
+class _FakeBatch:
+    """A batch whose window pressure follows p = -3 B (L / L_eq - 1) per replica; it
+    records the boxes it was built with."""
+    B_GPa = 200.0
+    built = []
+
+    def __init__(self, cells, L_eq):
+        from mdelast_b200.units import Units as U
+        self.cells, self.L_eq, self.U = cells, L_eq, U
+        self.n_replicas = len(cells)
+        _FakeBatch.built.append([float(c.box[0]) for c in cells])
+
+    def autotune(self, n):
+        return {}
+
+    def run(self, *a):
+        pass
+
+    def fluctuation_start(self):
+        pass
+
+    def set_sample_ring(self, n):
+        pass
+
+    def drain_samples(self, r):
+        p = -3.0 * self.B_GPa * (self.cells[r].box[0] / self.L_eq[r] - 1.0)
+        return {"pressure": np.full(4, p * self.U.GPa)}
+
+    def atoms(self, r, field):
+        c = self.cells[r]
+        return c.positions / c.box if field == "coords" else c.velocities
+
+    def chain(self, r, which):
+        return None, self.cells[r].thermo_p_eta, None
+
+    def elastic_constants(self, r):
+        return {"C11": 1.0, "C12": 1.0, "C44": 1.0}
+
+
+def _warm(monkeypatch, bulk, offset):
+    import mdelast_b200.protocol as P
+    from mdelast_b200.warmstart import judge
+
+    class _M:
+        ATOM_COORDINATES, ATOM_VELOCITIES = "coords", "vel"
+
+    cells = [_cell(), _cell(L=12e-8)]
+    L_eq = [c.box[0] / (1.0 + offset) for c in cells]
+    _FakeBatch.built = []
+    monkeypatch.setattr(P, "make_batch", lambda m, t, cs, **k: _FakeBatch(cs, L_eq))
+    fell_back = []
+
+    def fake_protocol(*a, **k):
+        fell_back.append(True)
+        return ProtocolResult("mixed", 2, 8, Stages(), [1.0, 1.0], [0.0, 0.0], {}, [])
+
+    monkeypatch.setattr(P, "run_protocol", fake_protocol)
+    st = Stages(0, 0, 100, 400, 5, 20, 200)
+    res = P.run_warm_start(_M, _Tables, cells, stages=st, judge=judge, check_steps=100,
+                           bulk_GPa=bulk, autotune=False)
+    return res, fell_back, L_eq
+
+
+def test_warm_start_corrects_the_box_from_the_window_pressure(monkeypatch):
+    # 0.1% too large an edge: the window reads -0.6 GPa, outside the 0.2 GPa tolerance;
+    # one Newton step with the right bulk modulus lands on the equilibrium box
+    res, fell_back, L_eq = _warm(monkeypatch, [200.0, 200.0], 1e-3)
+    assert not fell_back and res.accepted_start and res.corrections == 1
+    assert len(_FakeBatch.built) == 2
+    assert np.allclose(_FakeBatch.built[1], L_eq, rtol=2e-6)
+    assert all(abs(p) < 0.01 for p in res.npt_pressure_GPa)
+
+
+def test_warm_start_without_bulk_moduli_falls_back(monkeypatch):
+    res, fell_back, _ = _warm(monkeypatch, None, 1e-3)
+    assert fell_back and not res.accepted_start and res.corrections == 0
+
+
+def test_warm_start_accepts_a_good_box_untouched(monkeypatch):
+    res, fell_back, _ = _warm(monkeypatch, [200.0, 200.0], 1e-5)
+    assert not fell_back and res.corrections == 0 and len(_FakeBatch.built) == 1
+
+
+def test_born_stability_and_linear_guess():
+    from mdelast_b200.warmstart import _nialco_guess, born_stable, nialco_guess_a
+    ok = born_stable([250, 100, 250, 250], [150, 120, 150, -200], [90, 50, -1, 90])
+    assert ok.tolist() == [True, False, False, False]
+    x = np.array([[1.0, 0.0, 0.0], [0.2, 0.1, 0.7]])
+    g = _nialco_guess(x, [300.0, 600.0])
+    assert g[0] == nialco_guess_a(x[0], 300.0) and g[1] == nialco_guess_a(x[1], 600.0)
+    assert abs(g[0] - 3.52) < 1e-12
