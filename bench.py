@@ -121,8 +121,8 @@ def run_ours(args, rank, world, local_rank):
         import torch.distributed as dist
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
-    t, base = make_cells(1)
-    cells = make_cells(args.replicas, seed0=1000 * rank)[1]
+    t, base = make_cells(1, workload=args.workload)
+    cells = make_cells(args.replicas, seed0=1000 * rank, workload=args.workload)[1]
     N = base[0].n_atoms
     peaks = {}
     pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -138,8 +138,15 @@ def run_ours(args, rank, world, local_rank):
     # larger than the 126 MB L2 for 16 replicas, so steps run back to back unflushed.
     b = make_batch(m, t, cells, dt=DT, r_skin=SKIN, precision=args.precision,
                    device=local_rank)
-    # launch shapes of the pair passes timed on this workload and kept (setup, untimed)
-    tune = b.autotune(3)
+    # launch shapes of the pair passes timed on this workload and kept (setup, untimed),
+    # or the shapes given by --launch
+    if args.launch:
+        tpa_d, tpa_f, blk_d, blk_f = (int(v) for v in args.launch.split(","))
+        b.set_launch(tpa_d, tpa_f, blk_d, blk_f)
+        tune = {"tpa_density": tpa_d, "tpa_force": tpa_f, "blocks_density": blk_d,
+                "blocks_force": blk_f, "given": True}
+    else:
+        tune = b.autotune(3)
     b.run(args.warmup, REBUILD, 1, False)
     b.synchronize()
     barrier()
@@ -165,7 +172,8 @@ def run_ours(args, rank, world, local_rank):
     roof = {"bound": "hbm", "kernel": "k_force" + ("_mx" if args.precision == "mixed" else ""),
             "achieved": achieved, "peak": peak, "unit": "GB/s",
             "peak_source": "measured" if hbm else "fallback", "frac": achieved / peak,
-            "traffic": TRAFFIC_PER_LAUNCH.get((args.precision, args.replicas)),
+            "traffic": TRAFFIC_PER_LAUNCH.get((args.precision, args.replicas))
+            if args.workload == WORKLOAD else None,
             "algorithmic_bytes_per_launch": bytes_force, "half_list_nbar": nbar,
             "kernel_ms": {n: float(x) for n, x in zip(KERNELS, kt)}}
     del b
@@ -223,7 +231,7 @@ def run_ours(args, rank, world, local_rank):
     d2h = e2e_steps * args.replicas * (78 * 8 + 8) + args.replicas * 2 * N * 24
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == WORKLOAD:
         cpu = cpu_sample(N)
     cij = None
     if rank == 0 and not args.no_cij:
@@ -240,9 +248,10 @@ def run_ours(args, rank, world, local_rank):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if args.precision == "fp64" else "f32 pair math, f64 sums and integrator",
         "data": "synthetic (seeded FCC lattice and Zn placement, Maxwell-Boltzmann velocities)",
-        "config": {"workload": WORKLOAD, "atoms_per_replica": N,
+        "config": {"workload": args.workload, "atoms_per_replica": N,
                    "replicas_per_gpu": args.replicas, "atoms_per_gpu": N * args.replicas,
-                   "potential": "ZnCu.eam.alloy", "ensemble": "NVT 300 K", "dt_fs": 2,
+                   "potential": "ZnCu.eam.alloy", "ensemble": WORKLOADS[args.workload],
+                   "dt_fs": 2,
                    "neighbor_list": f"r_skin {SKIN}, rebuilt every {REBUILD} steps",
                    "sample_observables": "every step", "precision": args.precision,
                    "l2": ("inputs larger than L2 (replica state > 126 MB)"
@@ -290,17 +299,25 @@ def other_configs(m, t, device, steps=50, warmup=5):
     return out
 
 
-def make_cells(replicas, seed0=0):
-    """The workload cell (15x15x15 Cu-6 at.% Zn) in `replicas` copies that differ in their
-    velocity seed."""
+WORKLOADS = {WORKLOAD: "NVT 300 K", "l12_cuzn3_20x20x20_32000_nvt5": "NVT 5 K"}
+
+
+def make_cells(replicas, seed0=0, workload=WORKLOAD):
+    """The workload cell in `replicas` copies that differ in their velocity seed: the
+    15x15x15 Cu-6 at.% Zn cell (default), or the ordered L1_2 CuZn3 20x20x20 cell at
+    5 K."""
     from mdelast_b200.potentials import find_potential, read_setfl
-    from mdelast_b200.systems import cuzn_cell
+    from mdelast_b200.systems import cuzn_cell, l12_cell
     path = find_potential("ZnCu.eam.alloy")
     if path is None:
         raise SystemExit("ZnCu.eam.alloy not found (make -C oracle potentials)")
     t = read_setfl(path)
-    cells = [cuzn_cell(t, NSIDE, n_zn=N_ZN, T=T_K, ensemble=1, placement_seed=42,
-                       velocity_seed=seed0 + k) for k in range(replicas)]
+    if workload == WORKLOAD:
+        cells = [cuzn_cell(t, NSIDE, n_zn=N_ZN, T=T_K, ensemble=1, placement_seed=42,
+                           velocity_seed=seed0 + k) for k in range(replicas)]
+    else:
+        cells = [l12_cell(t, 20, T=5.0, ensemble=1, velocity_seed=500 + seed0 + k)
+                 for k in range(replicas)]
     return t, cells
 
 
@@ -534,6 +551,12 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--replicas", type=int, default=16)
     ap.add_argument("--precision", choices=("fp64", "mixed"), default="mixed")
+    ap.add_argument("--launch", default=None, metavar="TPA_D,TPA_F,BLOCKS_D,BLOCKS_F",
+                    help="launch shapes of the density and force passes instead of the "
+                         "autotuner's (lanes per atom, target block count)")
+    ap.add_argument("--workload", choices=tuple(WORKLOADS), default=WORKLOAD,
+                    help="the timed batch's cell (the C_ij comparisons always use the "
+                         "Cu-Zn cell)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")

@@ -99,9 +99,13 @@ struct TablesView {
     double eam_rcut[kMaxTypes];
     double rhomax[kMaxTypes];
     double mass[kMaxTypes];
-    // mixed precision: the r bundles in FP32 with lengths in angstrom and values in eV
-    // (phi) or angstrom^-3 (rho); cutoffs in angstrom
-    const float *rbf;
+    // mixed precision: the r tables in FP32 with lengths in angstrom and values in eV
+    // (phi) or angstrom^-3 (rho). rbf: per type pair (a <= b) and interval one record of
+    // TabFmt<IP>::kB floats holding phi_ab, rho_a, rho_b at strides of kFb (the force
+    // pass reads all three at one r, from one place); rrf: per type and interval one
+    // record of kFf floats holding rho (the density pass reads one function per pair).
+    // Cutoffs in angstrom.
+    const float *rbf, *rrf;
     float finv_hr, finv_hr2, fr_cut_sq, fpad;
     float fpot_rcut[kMaxTypes * (kMaxTypes + 1) / 2];
     float fpot_rmin[kMaxTypes * (kMaxTypes + 1) / 2];
@@ -213,6 +217,14 @@ __device__ __forceinline__ void ld6(const double *p, double c[6]) {
 // a pair-table bundle holds three functions (phi_ab, rho_a, rho_b).
 template <int IP> struct TabFmt {
     static constexpr int kF = IP == MDELAST_BSPLINE ? 12 : 6;
+    // FP32 records of the mixed-precision tables. The rho table pads a quintic's 6
+    // coefficients to 8 floats (one 32-byte sector, loaded as float4 + float2); the pair
+    // bundle keeps them packed (3 x 24 = 72 bytes), since the force pass is limited by how
+    // much of the table the L1 cache holds (measured: 96- and 128-byte bundles are 7 % and
+    // 19 % slower).
+    static constexpr int kFf = IP == MDELAST_BSPLINE ? 12 : 8;
+    static constexpr int kFb = IP == MDELAST_BSPLINE ? 12 : 6;
+    static constexpr int kB = 3 * kFb;
 };
 
 __device__ __forceinline__ double cubic_at(const double *p, double t) {

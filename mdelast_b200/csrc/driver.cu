@@ -131,7 +131,7 @@ struct mdelast_driver_s {
     int precision = MDELAST_PRECISION_FP64;
     float4 *d_posf = nullptr;
     float2 *d_dF2f = nullptr;
-    float *d_rbf = nullptr;
+    float *d_rbf = nullptr, *d_rrf = nullptr;
     void pass_density(bool obs, cudaStream_t s) {
         if (precision == MDELAST_PRECISION_MIXED)
             launch_density_mx(obs, tpa_d, grid_d, s, A, T);
@@ -234,6 +234,7 @@ mdelast_driver_s::~mdelast_driver_s() {
     dfree(d_posf);
     dfree(d_dF2f);
     dfree(d_rbf);
+    dfree(d_rrf);
     dfree(d_nbr);
     dfree(d_nup);
     dfree(d_ndn);
@@ -913,25 +914,45 @@ static int create_system(const mdelast_driver_config *cfgs, int n_rep, mdelast_d
     }
     d->precision = c0.precision;
     if (c0.precision == MDELAST_PRECISION_MIXED) {
-        // the r bundles in FP32, angstrom / eV (phi) and angstrom^-3 (rho). Quintic
+        // The r tables in FP32, angstrom / eV (phi) and angstrom^-3 (rho): per type pair
+        // and interval a bundle of phi_ab, rho_a, rho_b; per type and interval rho. Quintic
         // coefficients carry the function's unit (derivatives come with 1/h in angstrom);
-        // the bspline cubics of f' and f'' carry one and two more 1/length
-        std::vector<float> rbf(rb.size());
+        // the bspline cubics of f' and f'' carry one and two more 1/length.
+        size_t const kFf = bsp ? 12 : 8, kFb = bsp ? 12 : 6, kB = 3 * kFb;
         double const a3 = kAng * kAng * kAng;
-        for (size_t q = 0; q < rb.size(); ++q) {
-            size_t const w = q % (3 * kF);
-            double f = w < kF ? 1. / kEv : a3;
-            if (bsp) {
-                int const deriv = static_cast<int>((w % kF) / 4); // 0 f, 1 f', 2 f''
-                for (int d = 0; d < deriv; ++d)
+        auto pack = [&](const double *src, double unit, float *dst) {
+            for (size_t c = 0; c < kF; ++c) {
+                double f = unit;
+                for (size_t q = 0; bsp && q < c / 4; ++q) // 0 f, 1 f', 2 f''
                     f *= kAng;
+                dst[c] = static_cast<float>(src[c] * f);
             }
-            rbf[q] = static_cast<float>(rb[q] * f);
-        }
+        };
+        std::vector<float> rbf(static_cast<size_t>(npot) * nri * kB, 0.f);
+        std::vector<float> rrf(static_cast<size_t>(nt) * nri * kFf, 0.f);
+        for (int b = 0; b < nt; ++b)
+            for (int a = 0; a <= b; ++a) {
+                int const s = b * (b + 1) / 2 + a;
+                for (int k = 0; k < nri; ++k) {
+                    float *o = rbf.data() + (static_cast<size_t>(s) * nri + k) * kB;
+                    pack(fun(c0.pair[s]->table, k), 1. / kEv, o);
+                    if (c0.n_eam) {
+                        pack(fun(c0.eam[a]->rho, k), a3, o + kFb);
+                        pack(fun(c0.eam[b]->rho, k), a3, o + 2 * kFb);
+                    }
+                }
+            }
+        for (int t = 0; t < c0.n_eam; ++t)
+            for (int k = 0; k < nri; ++k)
+                pack(fun(c0.eam[t]->rho, k), a3,
+                     rrf.data() + (static_cast<size_t>(t) * nri + k) * kFf);
         TRY(dalloc(&d->d_rbf, rbf.size()));
-        if (cudaMemcpy(d->d_rbf, rbf.data(), sizeof(float) * rbf.size(), cudaMemcpyHostToDevice))
+        TRY(dalloc(&d->d_rrf, rrf.size()));
+        if (cudaMemcpy(d->d_rbf, rbf.data(), sizeof(float) * rbf.size(), cudaMemcpyHostToDevice) ||
+            cudaMemcpy(d->d_rrf, rrf.data(), sizeof(float) * rrf.size(), cudaMemcpyHostToDevice))
             return bail(fail(MDELAST_ERR_CUDA, "table upload failed"));
         T.rbf = d->d_rbf;
+        T.rrf = d->d_rrf;
         T.finv_hr = static_cast<float>(T.inv_hr * kAng);
         T.finv_hr2 = static_cast<float>(T.inv_hr2 * kAng * kAng);
         T.fr_cut_sq = static_cast<float>((rcut / kAng) * (rcut / kAng));

@@ -28,15 +28,28 @@ __device__ __forceinline__ int tab_locate_f(float x, float inv_h, int n, float &
     return i;
 }
 
-__device__ __forceinline__ void ld6f(const float *p, float c[6]) {
-    const float2 *q = reinterpret_cast<const float2 *>(p);
-    float2 a = __ldg(q), b = __ldg(q + 1), d = __ldg(q + 2);
-    c[0] = a.x;
-    c[1] = a.y;
-    c[2] = b.x;
-    c[3] = b.y;
-    c[4] = d.x;
-    c[5] = d.y;
+// the 6 quintic coefficients of a record: 16-byte aligned (PAD, the rho table's 8-float
+// records) or 8-byte aligned (the packed pair bundle)
+template <bool PAD> __device__ __forceinline__ void ld6f(const float *p, float c[6]) {
+    if constexpr (PAD) {
+        float4 const a = __ldg(reinterpret_cast<const float4 *>(p));
+        float2 const b = __ldg(reinterpret_cast<const float2 *>(p + 4));
+        c[0] = a.x;
+        c[1] = a.y;
+        c[2] = a.z;
+        c[3] = a.w;
+        c[4] = b.x;
+        c[5] = b.y;
+    } else {
+        const float2 *q = reinterpret_cast<const float2 *>(p);
+        float2 const a = __ldg(q), b = __ldg(q + 1), d = __ldg(q + 2);
+        c[0] = a.x;
+        c[1] = a.y;
+        c[2] = b.x;
+        c[3] = b.y;
+        c[4] = d.x;
+        c[5] = d.y;
+    }
 }
 
 // The pair force is evaluated from both of its atoms, in different code paths of the
@@ -65,7 +78,7 @@ __device__ __forceinline__ float cubicf_at(const float *p, float t) {
     return __fmaf_rn(t, __fmaf_rn(t, __fmaf_rn(t, a.w, a.z), a.y), a.x);
 }
 
-template <int IP, bool NV, bool ND1, bool ND2>
+template <int IP, bool NV, bool ND1, bool ND2, bool PAD = false>
 __device__ __forceinline__ void tabf_eval(const float *p, float t, float inv_h, float inv_h2,
                                           float &v, float &d1, float &d2) {
     if constexpr (IP == MDELAST_BSPLINE) {
@@ -77,7 +90,7 @@ __device__ __forceinline__ void tabf_eval(const float *p, float t, float inv_h, 
             d2 = cubicf_at(p + 8, t);
     } else {
         float c[6];
-        ld6f(p, c);
+        ld6f<PAD>(p, c);
         if (NV)
             v = tabf_v(c, t);
         if (ND1)
@@ -182,11 +195,10 @@ __global__ void __launch_bounds__(kBlock) k_density_mx(AtomsView A, TablesView T
                     continue;
                 float t;
                 int const k = tab_locate_f(dr, T.finv_hr, T.nri, t);
-                int const off = (tj == (ti < tj ? ti : tj)) ? kF : 2 * kF;
                 float v = 0.f, d1 = 0.f, d2 = 0.f;
-                tabf_eval<IP, true, OBS, false>(
-                    T.rbf + (static_cast<size_t>(pair_slot(ti, tj)) * T.nri + k) * 3 * kF + off,
-                    t, T.finv_hr, T.finv_hr2, v, d1, d2);
+                tabf_eval<IP, true, OBS, false, true>(
+                    T.rrf + (static_cast<size_t>(tj) * T.nri + k) * TabFmt<IP>::kFf, t,
+                    T.finv_hr, T.finv_hr2, v, d1, d2);
                 rho += v;
                 if (OBS) {
                     float const ar = d1 * idr;
@@ -321,8 +333,8 @@ __device__ __forceinline__ void force_row_mx(AtomsView const &A, TablesView cons
         int const s = pair_slot(ti, tj);
         float t;
         int const k = tab_locate_f(dr, T.finv_hr, T.nri, t);
-        constexpr int kF = TabFmt<IP>::kF;
-        const float *bundle = T.rbf + (static_cast<size_t>(s) * T.nri + k) * 3 * kF;
+        constexpr int kFb = TabFmt<IP>::kFb;
+        const float *bundle = T.rbf + (static_cast<size_t>(s) * T.nri + k) * TabFmt<IP>::kB;
         float V = 0.f, dV = 0.f, d2V = 0.f;
         if (dr < T.fpot_rmin[s])
             warn_rmin = true;
@@ -334,7 +346,8 @@ __device__ __forceinline__ void force_row_mx(AtomsView const &A, TablesView cons
             lap = 2.f * (d2V + 2.f * dV * idr);
         }
         if (T.has_eam) {
-            int const oi = (ti <= tj) ? kF : 2 * kF, oj = (ti < tj) ? 2 * kF : kF;
+            // rho'_{t_i} and rho'_{t_j} at r: rho_a of the bundle belongs to the smaller type
+            int const oi = (ti <= tj) ? kFb : 2 * kFb, oj = (ti < tj) ? 2 * kFb : kFb;
             float drho_i = 0.f, drho_j = 0.f, d2rho_i = 0.f, d2rho_j = 0.f, unused = 0.f;
             if (!(dr > T.feam_rcut[ti]))
                 tabf_eval<IP, false, true, OBS>(bundle + oi, t, T.finv_hr, T.finv_hr2, unused,
