@@ -239,7 +239,7 @@ def run_ours(args, rank, world, local_rank):
     cij_nialco = None
     if rank == 0 and args.cij_nialco:
         cij_nialco = time_to_cij_nialco(m)
-    others = None if args.no_configs else other_configs(m, t, local_rank)
+    others = None if args.no_configs else other_configs(m, t, local_rank, peak=peak)
     n_rebuilds = (args.steps + REBUILD - 1) // REBUILD
     launches = args.steps * 6 + n_rebuilds * 3
     line = {
@@ -263,6 +263,7 @@ def run_ours(args, rank, world, local_rank):
         "time_to_cij_nialco_108000": cij_nialco,
         "other_configs": others,
         "roofline": roof,
+        "roofline_step": step_roofline(value / world, nbar, peak),
         "cpu_baseline": cpu,
         "e2e": None if args.no_e2e else {
             "value": e2e_value, "unit": "atom-steps/s",
@@ -279,7 +280,27 @@ def run_ours(args, rank, world, local_rank):
         dist.destroy_process_group()
 
 
-def other_configs(m, t, device, steps=50, warmup=5):
+def step_roofline(value, nbar, peak, sampled=True):
+    """Whole-step HBM roofline: B = 8 nbar + 144 bytes per atom-step (list indices read by
+    both pair passes, positions, types, F', velocities, positions written), plus 152 on
+    sampled steps (g, h and F''), with nbar the reference's half-list entries per atom."""
+    b = 8.0 * nbar + 144.0 + (152.0 if sampled else 0.0)
+    achieved = value * b / 1e9
+    return {"bound": "hbm", "bytes_per_atom_step": b, "half_list_nbar": nbar,
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak}
+
+
+def batch_nbar(b):
+    """Half-list entries per atom over all replicas of a batch (its current list)."""
+    tot = n = 0
+    for r in range(b.n_replicas):
+        point, _ = b.neighbor_list(r)
+        tot += int(point[-1])
+        n += len(point) - 1
+    return tot / n
+
+
+def other_configs(m, t, device, steps=50, warmup=5, peak=6650.0):
     """Atom-steps/s of the other batched and single-cell workloads, mixed precision,
     observables every step, list rebuilt every 20 steps, autotuned, CUDA-event timed:
     64 uneven replicas (4 n^3 atoms, n uniform in [4, 20], x_Zn in [0, 0.3], T in [5, 900] K,
@@ -292,9 +313,11 @@ def other_configs(m, t, device, steps=50, warmup=5):
         tune = b.autotune(2)
         b.run(warmup, REBUILD, 1, False)
         ms = b.run(steps, REBUILD, 1, True)
-        out[name] = {"value": b.n_atoms * steps / (ms * 1e-3), "unit": "atom-steps/s",
+        value = b.n_atoms * steps / (ms * 1e-3)
+        out[name] = {"value": value, "unit": "atom-steps/s",
                      "atoms": b.n_atoms, "replicas": b.n_replicas, "steps": steps,
-                     "ms_per_step": ms / steps, "launch": tune}
+                     "ms_per_step": ms / steps, "launch": tune,
+                     "roofline_step": step_roofline(value, batch_nbar(b), peak)}
         del b
     return out
 
@@ -462,9 +485,10 @@ def half_list_nbar(m, t, cell):
 
 
 # ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_force_mx launch
-# (profiles/k_force_mx_k_density_mx_bench_4x13500.md, 4 replicas, cold caches); the
-# 16- and 32-replica entries scale it by the atoms processed. None where not captured.
-_TRAFFIC_4 = 53.211904e6 + 0.262656e6
+# (profiles/k_force_mx_k_density_mx_bench_4x13500.md, 4 replicas, the 200th step, cold
+# caches); the 16- and 32-replica entries scale it by the atoms processed. None where not
+# captured.
+_TRAFFIC_4 = 39.514624e6 + 0.032512e6
 TRAFFIC_PER_LAUNCH: dict = {("mixed", 4): _TRAFFIC_4, ("mixed", 16): 4 * _TRAFFIC_4,
                             ("mixed", 32): 8 * _TRAFFIC_4}
 

@@ -747,6 +747,19 @@ class BatchedMDDriver {
         check(mdelast_batch_get_status(d_, a.mutable_data()));
         return a;
     }
+    // replica r's half list (md_driver.cpp:279-298) as CSR (point, neighbors)
+    py::tuple neighbor_list(int r) {
+        if (r < 0 || r >= n_replicas())
+            throw py::index_error("replica index out of range");
+        size_t const N = counts_[static_cast<size_t>(r)];
+        py::array_t<int32_t> point(N + 1);
+        int64_t total = 0;
+        check(mdelast_batch_get_neighbors(d_, r, point.mutable_data(), nullptr, 0, &total));
+        py::array_t<int32_t> nb(static_cast<size_t>(total));
+        check(mdelast_batch_get_neighbors(d_, r, point.mutable_data(), nb.mutable_data(), total,
+                                          &total));
+        return py::make_tuple(point, nb);
+    }
     py::array_t<double> atoms(int r, int field) {
         if (r < 0 || r >= n_replicas())
             throw py::index_error("replica index out of range");
@@ -1007,6 +1020,7 @@ PYBIND11_MODULE(md_driver_module, m) {
         .def("observables", &BatchedMDDriver::observables, py::arg("replica"))
         .def("status", &BatchedMDDriver::status)
         .def("atoms", &BatchedMDDriver::atoms, py::arg("replica"), py::arg("field"))
+        .def("neighbor_list", &BatchedMDDriver::neighbor_list, py::arg("replica"))
         .def("kernel_times", &BatchedMDDriver::kernel_times, py::arg("n_steps") = 10)
         .def("autotune", &BatchedMDDriver::autotune, py::arg("n_repeat") = 3)
         .def("set_launch", &BatchedMDDriver::set_launch, py::arg("tpa_density"),
