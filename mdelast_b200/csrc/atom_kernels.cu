@@ -123,14 +123,23 @@ __device__ __forceinline__ void nb_batch(AtomsView const &A, int i, int j, bool 
 // order as the per-atom search, so the same list, without re-gathering every candidate
 // from global memory for each atom of the cell. Replicas whose box has shrunk below the
 // cell grid (reach > 1) are left to k_nbr_build.
+//
+// Most staged candidates (about 7 in 8) lie well outside the list radius. Each is first
+// tested in FP32 on wrapped scaled coordinates with a margin that covers the FP32 error
+// (so no pair within the radius is dropped); the survivors are packed, in candidate order,
+// into a per-warp queue and get the reference's exact FP64 test 32 at a time, with every
+// lane busy. The pairs kept and their order are those of the plain FP64 search.
 constexpr int kStage = 512;
+constexpr int kWarps = 4; // warps per block of k_nbr_cells
 
 __global__ void __launch_bounds__(128) k_nbr_cells(AtomsView A) {
     extern __shared__ unsigned char s_raw[];
     double4 *s_c = reinterpret_cast<double4 *>(s_raw);
-    int *s_j = reinterpret_cast<int *>(s_c + kStage);
+    float4 *s_w = reinterpret_cast<float4 *>(s_c + kStage); // wrapped scaled, FP32
+    int *s_j = reinterpret_cast<int *>(s_w + kStage);
     int *s_cnt = s_j + kStage;    // [4][cell_cap]: nu, nd, total, full of the cell's atoms
     __shared__ int s_cell[27], s_off[28];
+    __shared__ int s_queue[kWarps][64]; // staged indices that passed the FP32 test
     int const cell = blockIdx.x;
     int const r = A.cell_rep[cell];
     Replica const &R = A.rep[r];
@@ -168,6 +177,15 @@ __global__ void __launch_bounds__(128) k_nbr_cells(AtomsView A) {
     int const warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     double const hx = R.h[0], hy = R.h[1], hz = R.h[2];
     double const rl2 = A.r_list_sq;
+    // FP32 pre-test: |w| <= 1/2 carries at most 2^-26 of rounding per coordinate, the
+    // difference at most 3 2^-26 before the scaling by h; 1e-7 (h_x + h_y + h_z) and a
+    // 1e-6 relative widening of the radius cover that and the FP32 products and sums.
+    float const hxf = static_cast<float>(hx), hyf = static_cast<float>(hy),
+                hzf = static_cast<float>(hz);
+    double const rpre = sqrt(rl2) * (1. + 1e-6) + 1e-7 * (hx + hy + hz);
+    float const rpre2 = static_cast<float>(rpre * rpre * (1. + 1e-6));
+    int *queue = s_queue[warp];
+    unsigned const lt = (1u << lane) - 1u;
     for (int c0 = 0; c0 < M; c0 += kStage) {
         int const len = min(kStage, M - c0);
         for (int t = threadIdx.x; t < len; t += blockDim.x) {
@@ -177,23 +195,61 @@ __global__ void __launch_bounds__(128) k_nbr_cells(AtomsView A) {
                 ++q;
             int const j = A.cell_atoms[static_cast<size_t>(s_cell[q]) * cap + (g - s_off[q])];
             s_j[t] = j;
-            s_c[t] = A.crd[j];
+            double4 const c = A.crd[j];
+            s_c[t] = c;
+            s_w[t] = make_float4(static_cast<float>(c.x - nint_ref(c.x)),
+                                 static_cast<float>(c.y - nint_ref(c.y)),
+                                 static_cast<float>(c.z - nint_ref(c.z)), 0.f);
         }
         __syncthreads();
         for (int a = warp; a < n_me; a += nwarp) {
             int const i = me[a];
             double4 const ci = A.crd[i];
+            float const wx = static_cast<float>(ci.x - nint_ref(ci.x)),
+                        wy = static_cast<float>(ci.y - nint_ref(ci.y)),
+                        wz = static_cast<float>(ci.z - nint_ref(ci.z));
             int nu = c_nu[a], nd = c_nd[a], total = c_tot[a];
             bool full = c_full[a] != 0;
-            for (int base = 0; base < len; base += 32) {
-                int const k = base + static_cast<int>(lane);
-                int const j = k < len ? s_j[k] : -1;
+            // exact test of the first n (<= 32) queued candidates, one per lane in order
+            auto drain = [&](int n) {
+                int const k = static_cast<int>(lane) < n ? queue[lane] : -1;
+                int const j = k >= 0 ? s_j[k] : -1;
                 bool hit = false;
-                if (k < len && j != i) {
+                if (k >= 0) {
                     double px, py, pz;
                     hit = min_image_r2(ci, s_c[k], hx, hy, hz, px, py, pz) <= rl2;
                 }
                 nb_batch(A, i, j, hit, lane, nu, nd, total, full);
+            };
+            int pend = 0;
+            for (int base = 0; base < len; base += 32) {
+                int const k = base + static_cast<int>(lane);
+                bool pass = false;
+                if (k < len && s_j[k] != i) {
+                    float4 const w = s_w[k];
+                    float dx = wx - w.x, dy = wy - w.y, dz = wz - w.z;
+                    dx = (dx - rintf(dx)) * hxf;
+                    dy = (dy - rintf(dy)) * hyf;
+                    dz = (dz - rintf(dz)) * hzf;
+                    pass = dx * dx + dy * dy + dz * dz <= rpre2;
+                }
+                unsigned const bal = __ballot_sync(0xffffffffu, pass);
+                if (pass)
+                    queue[pend + __popc(bal & lt)] = k;
+                pend += __popc(bal);
+                __syncwarp();
+                if (pend >= 32) {
+                    drain(32);
+                    __syncwarp();
+                    if (static_cast<int>(lane) < pend - 32)
+                        queue[lane] = queue[32 + lane];
+                    pend -= 32;
+                    __syncwarp();
+                }
+            }
+            if (pend > 0) {
+                drain(pend);
+                __syncwarp();
             }
             if (lane == 0) {
                 c_nu[a] = nu;
@@ -215,7 +271,8 @@ __global__ void __launch_bounds__(128) k_nbr_cells(AtomsView A) {
 }
 
 size_t nbr_cells_smem(int cell_cap) {
-    return (sizeof(double4) + sizeof(int)) * kStage + 4 * sizeof(int) * cell_cap;
+    return (sizeof(double4) + sizeof(float4) + sizeof(int)) * kStage +
+           4 * sizeof(int) * cell_cap;
 }
 
 // One warp per atom slot; the lanes test 32 candidates at a time. Atoms of cell-list
