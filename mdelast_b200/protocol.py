@@ -64,7 +64,8 @@ def _nvt_cells(tables, cells, positions, coordinates, V_V0, seeds, handoff):
     """Cells of the NVT stage in the NPT production-mean box L0 (V/V0)^(1/3).
 
     handoff "reference": the snapshot's positions times (V/V0)^(1/3), as
-    sample_case/run.py:273-279 does; the snapshot's positions are already in the NPT box,
+    sample_case/run.py:273-279 does, wrapped into the mean box as
+    benchmarks/l12_cuzn3_5K/run.py:127-140 does; the snapshot's positions are already in the NPT box,
     so the lattice is stretched a second time and squeezed at the periodic boundary (a
     misfit that takes the NVT stage tens of picoseconds to anneal). "box": the snapshot's
     scaled coordinates placed in the mean box. Both draw fresh velocities and chain
@@ -75,7 +76,10 @@ def _nvt_cells(tables, cells, positions, coordinates, V_V0, seeds, handoff):
         scale = v ** (1.0 / 3.0)
         L = c.box * scale
         if handoff == "reference":
+            # scaled, then wrapped into the mean box as benchmarks/l12_cuzn3_5K/run.py:127-140
+            # does (x >= L/2 moves down by L, x < -L/2 up by L)
             pos, _ = handoff_positions(positions[k][0], v)
+            pos = pos - L * np.floor((pos + 0.5 * L) / L)
         else:
             u = np.asarray(coordinates[k], dtype=float)
             pos = (u - np.floor(u + 0.5)) * L

@@ -44,10 +44,18 @@ def test_continue_handoff_carries_velocities_and_chain():
 
 
 def test_reference_handoff_is_the_scripts_arithmetic():
-    c = _cell()
-    p = c.positions * 1.01
+    c = _cell(n=64)
+    p = c.positions * 1.05  # a snapshot in a box 5 % larger than the mean box
     (nv,) = _nvt_cells(_Tables, [c], [(p, None, None)], [None], [1.0303], [7], "reference")
-    assert np.array_equal(nv.positions, handoff_positions(p, 1.0303)[0])
+    q = handoff_positions(p, 1.0303)[0]
+    L = nv.box
+    inside = np.all(np.abs(q) < 0.5 * L, axis=1)
+    assert inside.any() and not inside.all()
+    # scaled positions kept where inside the mean box, wrapped by one edge where not
+    assert np.array_equal(nv.positions[inside], q[inside])
+    out = ~inside
+    assert np.allclose(nv.positions[out], q[out] - L * np.round(q[out] / L), rtol=0, atol=1e-20)
+    assert np.all(nv.positions >= -0.5 * L) and np.all(nv.positions < 0.5 * L)
 
 
 def test_time_to_within_needs_to_stay_inside():
