@@ -494,8 +494,10 @@ TRAFFIC_PER_LAUNCH: dict = {("mixed", 4): _TRAFFIC_4, ("mixed", 16): 4 * _TRAFFI
 
 
 # ----------------------------------------------------------------------------- reference
-def _ref_worker(n_steps):
-    """One host process: the reference's C++ core on the workload cell; returns s/step."""
+def _ref_worker(args):
+    """One host process: the reference's C++ core on the workload cell, n_warm untimed
+    steps then one list build and n_steps timed steps; returns s/step (list amortised)."""
+    n_steps, n_warm = args
     sys.path.insert(0, ROOT)
     os.dup2(os.open(os.devnull, os.O_WRONLY), 1)  # the reference prints from C++
     import numpy as np
@@ -509,6 +511,8 @@ def _ref_worker(n_steps):
                   baro=(c.pressure, c.baro_w, c.baro_p_eps),
                   baro_thermo=(c.T, c.baro_q, c.baro_p_eta, 1.0),
                   box=np.diag(c.box), rg=rg_bins(c), Nf=c.Nf, dt=DT, neighbors=True, r_skin=SKIN)
+    if n_warm > 0:
+        d.integrate(n_warm)
     t0 = time.perf_counter()
     d.calculate_neighbors()
     t_list = time.perf_counter() - t0
@@ -525,7 +529,7 @@ def cpu_sample(N, n_steps=8):
         return None
     ctx = mp.get_context("spawn")
     with ctx.Pool(1) as pool:
-        per_step = pool.map(_ref_worker, [n_steps])[0]
+        per_step = pool.map(_ref_worker, [(n_steps, 0)])[0]
     return {"value": N / per_step, "unit": "atom-steps/s", "cores": 1, "kind": "reference",
             "sample": f"{N}-atom workload cell: one list build + {n_steps} sampled steps, "
                       f"list cost amortised over {REBUILD} steps; {per_step * 1e3:.1f} ms/step"}
@@ -540,26 +544,29 @@ def run_reference(args, rank):
                           "oracle/_ref/libmdelast_ref.so not built (make -C oracle ref)"}))
         return
     cores = os.cpu_count() or 1
+    # a bounded sample per process: at most 10 timed steps after at most 10 warm-up steps
     n_steps = max(1, min(args.steps, 10))
+    n_warm = max(0, min(args.warmup, 10))
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
     with ctx.Pool(cores) as pool:
-        per_step = pool.map(_ref_worker, [n_steps] * cores)
+        per_step = pool.map(_ref_worker, [(n_steps, n_warm)] * cores)
     wall = time.perf_counter() - t0
     N = NSIDE**3 * 4
     value = sum(N / x for x in per_step)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "atom-steps/s",
-        "n_gpus": 0, "steps": n_steps, "warmup": 0,
+        "n_gpus": 0, "steps": n_steps, "warmup": n_warm,
+        "steps_requested": args.steps, "warmup_requested": args.warmup,
         "ms_per_step": statistics.mean(per_step) * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "atoms_per_replica": N, "replicas": cores,
                    "parallelism": f"{cores} independent single-thread processes"},
         "cpu_baseline": {"value": value, "unit": "atom-steps/s", "cores": cores,
                          "kind": "reference",
-                         "sample": f"per process: one O(N^2) list build + {n_steps} steps of "
-                                   f"the {N}-atom cell (list amortised over {REBUILD}); "
-                                   f"wall {wall:.1f} s"},
+                         "sample": f"per process: {n_warm} warm-up steps, then one O(N^2) list "
+                                   f"build + {n_steps} timed steps of the {N}-atom cell (list "
+                                   f"amortised over {REBUILD}); wall {wall:.1f} s"},
         "e2e": {"value": value, "unit": "atom-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
