@@ -258,6 +258,29 @@ __device__ int monomial_index(int iv, int ivp) {
     return 0;
 }
 
+// The replica state in shared memory for k_post: one thread works through a long chain of
+// dependent updates of it (the thermodynamics), and reading and writing it in global
+// memory on that chain costs a round trip to L2 per access. Copied in and out by the
+// whole block.
+__device__ __forceinline__ void replica_load(Replica const *g, Replica *s) {
+    static_assert(sizeof(Replica) % sizeof(double) == 0, "Replica is copied as doubles");
+    const double *src = reinterpret_cast<const double *>(g);
+    double *dst = reinterpret_cast<double *>(s);
+    for (int k = threadIdx.x; k < static_cast<int>(sizeof(Replica) / sizeof(double));
+         k += blockDim.x)
+        dst[k] = src[k];
+    __syncthreads();
+}
+
+__device__ __forceinline__ void replica_store(Replica const *s, Replica *g) {
+    __syncthreads();
+    const double *src = reinterpret_cast<const double *>(s);
+    double *dst = reinterpret_cast<double *>(g);
+    for (int k = threadIdx.x; k < static_cast<int>(sizeof(Replica) / sizeof(double));
+         k += blockDim.x)
+        dst[k] = src[k];
+}
+
 } // namespace
 
 // Opening scalar work of integrate() (md_driver.cpp:567-581): barostat and particle NHC
@@ -436,11 +459,17 @@ __global__ void k_samples_reset(AtomsView A, int what) {
     }
 }
 
+__device__ void thermodynamics(AtomsView const &A, Replica *R, int mode, int obs,
+                               const double *sf, const double *sd, double S, double ekin,
+                               double virial);
+
 __global__ void k_post(AtomsView A, int mode, int obs) {
-    Replica *R = A.rep + blockIdx.x;
+    __shared__ Replica sR;
     __shared__ double sf[F_NSUM], sd[D_NSUM];
     __shared__ double s_part[4][F_NSUM + D_NSUM];
     __shared__ double s_S, s_ekin, s_virial;
+    replica_load(A.rep + blockIdx.x, &sR);
+    Replica *R = &sR;
     int const t = threadIdx.x;
     // Chunk sums of the two passes (k_reduce): 4 groups of 64 threads, thread (g, q) adds
     // slot q over chunks g, g+4, ...; the group totals are then added in a fixed order, so
@@ -526,10 +555,19 @@ __global__ void k_post(AtomsView A, int mode, int obs) {
         s_S = 1.;
     }
     __syncthreads();
-    if (t != 0)
-        return;
-    // calculate_thermodynamics (md_driver.cpp:648-730)
-    double const S = s_S, ekin = s_ekin, virial = s_virial;
+    if (t == 0)
+        thermodynamics(A, R, mode, obs, sf, sd, s_S, s_ekin, s_virial);
+    replica_store(&sR, A.rep + blockIdx.x);
+}
+
+// calculate_thermodynamics (md_driver.cpp:648-730) and the sample record, on the replica's
+// shared copy
+__device__ void thermodynamics(AtomsView const &A, Replica *R, int mode, int obs,
+                               const double *sf, const double *sd, double S, double ekin,
+                               double virial) {
+    mdelast_observables &o = R->obs;
+    double const dt = R->dt;
+    int const ens = R->ensemble;
     int const N = R->n_atoms;
     R->vscale = S;
     o.ekin_tot = ekin;
