@@ -217,12 +217,11 @@ __device__ __forceinline__ void ld6(const double *p, double c[6]) {
 // a pair-table bundle holds three functions (phi_ab, rho_a, rho_b).
 template <int IP> struct TabFmt {
     static constexpr int kF = IP == MDELAST_BSPLINE ? 12 : 6;
-    // FP32 records of the mixed-precision tables. The rho table pads a quintic's 6
-    // coefficients to 8 floats (one 32-byte sector, loaded as float4 + float2); the pair
-    // bundle keeps them packed (3 x 24 = 72 bytes), since the force pass is limited by how
-    // much of the table the L1 cache holds (measured: 96- and 128-byte bundles are 7 % and
-    // 19 % slower).
-    static constexpr int kFf = IP == MDELAST_BSPLINE ? 12 : 8;
+    // FP32 records of the mixed-precision tables, packed (a quintic's 6 coefficients in 24
+    // bytes, 3 x 24 = 72 bytes per pair bundle): the pair passes are limited by how much of
+    // the tables the L1 cache holds (measured: 96- and 128-byte bundles make the force pass
+    // 7 % and 19 % slower; 32-byte rho records make the density pass 4.5 % slower).
+    static constexpr int kFf = IP == MDELAST_BSPLINE ? 12 : 6;
     static constexpr int kFb = IP == MDELAST_BSPLINE ? 12 : 6;
     static constexpr int kB = 3 * kFb;
 };

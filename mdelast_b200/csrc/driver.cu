@@ -918,7 +918,7 @@ static int create_system(const mdelast_driver_config *cfgs, int n_rep, mdelast_d
         // and interval a bundle of phi_ab, rho_a, rho_b; per type and interval rho. Quintic
         // coefficients carry the function's unit (derivatives come with 1/h in angstrom);
         // the bspline cubics of f' and f'' carry one and two more 1/length.
-        size_t const kFf = bsp ? 12 : 8, kFb = bsp ? 12 : 6, kB = 3 * kFb;
+        size_t const kFf = bsp ? 12 : 6, kFb = bsp ? 12 : 6, kB = 3 * kFb;
         double const a3 = kAng * kAng * kAng;
         auto pack = [&](const double *src, double unit, float *dst) {
             for (size_t c = 0; c < kF; ++c) {

@@ -28,28 +28,16 @@ __device__ __forceinline__ int tab_locate_f(float x, float inv_h, int n, float &
     return i;
 }
 
-// the 6 quintic coefficients of a record: 16-byte aligned (PAD, the rho table's 8-float
-// records) or 8-byte aligned (the packed pair bundle)
-template <bool PAD> __device__ __forceinline__ void ld6f(const float *p, float c[6]) {
-    if constexpr (PAD) {
-        float4 const a = __ldg(reinterpret_cast<const float4 *>(p));
-        float2 const b = __ldg(reinterpret_cast<const float2 *>(p + 4));
-        c[0] = a.x;
-        c[1] = a.y;
-        c[2] = a.z;
-        c[3] = a.w;
-        c[4] = b.x;
-        c[5] = b.y;
-    } else {
-        const float2 *q = reinterpret_cast<const float2 *>(p);
-        float2 const a = __ldg(q), b = __ldg(q + 1), d = __ldg(q + 2);
-        c[0] = a.x;
-        c[1] = a.y;
-        c[2] = b.x;
-        c[3] = b.y;
-        c[4] = d.x;
-        c[5] = d.y;
-    }
+// the 6 quintic coefficients of a packed (8-byte aligned) record
+__device__ __forceinline__ void ld6f(const float *p, float c[6]) {
+    const float2 *q = reinterpret_cast<const float2 *>(p);
+    float2 const a = __ldg(q), b = __ldg(q + 1), d = __ldg(q + 2);
+    c[0] = a.x;
+    c[1] = a.y;
+    c[2] = b.x;
+    c[3] = b.y;
+    c[4] = d.x;
+    c[5] = d.y;
 }
 
 // The pair force is evaluated from both of its atoms, in different code paths of the
@@ -78,7 +66,7 @@ __device__ __forceinline__ float cubicf_at(const float *p, float t) {
     return __fmaf_rn(t, __fmaf_rn(t, __fmaf_rn(t, a.w, a.z), a.y), a.x);
 }
 
-template <int IP, bool NV, bool ND1, bool ND2, bool PAD = false>
+template <int IP, bool NV, bool ND1, bool ND2>
 __device__ __forceinline__ void tabf_eval(const float *p, float t, float inv_h, float inv_h2,
                                           float &v, float &d1, float &d2) {
     if constexpr (IP == MDELAST_BSPLINE) {
@@ -90,7 +78,7 @@ __device__ __forceinline__ void tabf_eval(const float *p, float t, float inv_h, 
             d2 = cubicf_at(p + 8, t);
     } else {
         float c[6];
-        ld6f<PAD>(p, c);
+        ld6f(p, c);
         if (NV)
             v = tabf_v(c, t);
         if (ND1)
@@ -196,7 +184,7 @@ __global__ void __launch_bounds__(kBlock) k_density_mx(AtomsView A, TablesView T
                 float t;
                 int const k = tab_locate_f(dr, T.finv_hr, T.nri, t);
                 float v = 0.f, d1 = 0.f, d2 = 0.f;
-                tabf_eval<IP, true, OBS, false, true>(
+                tabf_eval<IP, true, OBS, false>(
                     T.rrf + (static_cast<size_t>(tj) * T.nri + k) * TabFmt<IP>::kFf, t,
                     T.finv_hr, T.finv_hr2, v, d1, d2);
                 rho += v;
