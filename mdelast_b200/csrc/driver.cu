@@ -156,6 +156,7 @@ struct mdelast_driver_s {
             k_sublist<<<n_pad / 8, 256, 0, s>>>(A);
     }
     double *d_pd = nullptr, *d_pf = nullptr, *d_red = nullptr;
+    size_t cap_dmap = 0, cap_fmap = 0, cap_pd = 0, cap_pf = 0, cap_red = 0; // elements
     // closing scalar work: fold the block sums, then the per-replica kernel
     void post(int mode, int obs, cudaStream_t s) {
         k_reduce<<<dim3(A.max_chunks, n_rep), 256, 0, s>>>(A);
@@ -374,20 +375,27 @@ int mdelast_driver_s::set_launch(int tpa_d_, int tpa_f_, int tgt_d, int tgt_f) {
     for (Replica const *x : reps)
         chunks = std::max(chunks, (std::max(x->dblk_n, x->fblk_n) + kChunk - 1) / kChunk);
     drop_graphs();
-    dfree(d_dblk_rep);
-    dfree(d_fblk_rep);
-    dfree(d_pd);
-    dfree(d_pf);
-    dfree(d_red);
-    if (int rc = dalloc(&d_dblk_rep, dmap.size()))
+    // grow the block maps and sums only: the autotuner tries many shapes in a row, and a
+    // free and an allocation per shape cost far more than the launches it times
+    auto grow = [](auto *&p, size_t &cap, size_t n) -> int {
+        if (n <= cap && p)
+            return MDELAST_OK;
+        dfree(p);
+        cap = 0;
+        if (int rc = dalloc(&p, n))
+            return rc;
+        cap = n;
+        return MDELAST_OK;
+    };
+    if (int rc = grow(d_dblk_rep, cap_dmap, dmap.size()))
         return rc;
-    if (int rc = dalloc(&d_fblk_rep, fmap.size()))
+    if (int rc = grow(d_fblk_rep, cap_fmap, fmap.size()))
         return rc;
-    if (int rc = dalloc(&d_pd, static_cast<size_t>(gd) * D_NSUM))
+    if (int rc = grow(d_pd, cap_pd, static_cast<size_t>(gd) * D_NSUM))
         return rc;
-    if (int rc = dalloc(&d_pf, static_cast<size_t>(gf) * F_NSUM))
+    if (int rc = grow(d_pf, cap_pf, static_cast<size_t>(gf) * F_NSUM))
         return rc;
-    if (int rc = dalloc(&d_red, static_cast<size_t>(n_rep) * chunks * 64))
+    if (int rc = grow(d_red, cap_red, static_cast<size_t>(n_rep) * chunks * 64))
         return rc;
     CK(cudaMemcpy(d_dblk_rep, dmap.data(), sizeof(int) * dmap.size(), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(d_fblk_rep, fmap.data(), sizeof(int) * fmap.size(), cudaMemcpyHostToDevice));
@@ -1026,6 +1034,8 @@ static int create_system(const mdelast_driver_config *cfgs, int n_rep, mdelast_d
     d->grid_f = deal_blocks(reps, d->tpa_f, false, fmap);
     TRY(dalloc(&d->d_dblk_rep, dmap.size()));
     TRY(dalloc(&d->d_fblk_rep, fmap.size()));
+    d->cap_dmap = dmap.size();
+    d->cap_fmap = fmap.size();
     TRY(dalloc(&d->d_rep, static_cast<size_t>(n_rep)));
     if (cudaMemcpy(d->d_rep, R.data(), sizeof(Replica) * n_rep, cudaMemcpyHostToDevice) ||
         cudaMemcpy(d->d_dblk_rep, dmap.data(), sizeof(int) * dmap.size(), cudaMemcpyHostToDevice) ||
@@ -1049,10 +1059,13 @@ static int create_system(const mdelast_driver_config *cfgs, int n_rep, mdelast_d
     TRY(dalloc(&d->d_ndn, np));
     TRY(dalloc(&d->d_pd, static_cast<size_t>(d->grid_d) * D_NSUM));
     TRY(dalloc(&d->d_pf, static_cast<size_t>(d->grid_f) * F_NSUM));
+    d->cap_pd = static_cast<size_t>(d->grid_d) * D_NSUM;
+    d->cap_pf = static_cast<size_t>(d->grid_f) * F_NSUM;
     int max_chunks = 1;
     for (Replica const *x : reps)
         max_chunks = std::max(max_chunks, (std::max(x->dblk_n, x->fblk_n) + kChunk - 1) / kChunk);
     TRY(dalloc(&d->d_red, static_cast<size_t>(n_rep) * max_chunks * 64));
+    d->cap_red = static_cast<size_t>(n_rep) * max_chunks * 64;
     TRY(dalloc(&d->d_max_count, 2));
     TRY(dalloc(&d->d_pos0, pos0.size()));
     int max_n = 0;

@@ -167,11 +167,11 @@ __global__ void __launch_bounds__(kBlock) k_density_mx(AtomsView A, TablesView T
             ti = static_cast<int>(pi.w);
             int const nu = A.pn_up[i], ntot = nu + A.pn_dn[i];
             int const *row = A.pnbr + static_cast<size_t>(i) * A.pmaxn;
-            float4 pn = A.posf[sub < ntot ? row[list_slot(sub, nu, A.pmaxn)] : i];
+            float4 pn = A.posf[sub < ntot ? __ldcs(row + list_slot(sub, nu, A.pmaxn)) : i];
             for (int kk = sub; kk < ntot; kk += TPA) {
                 float4 const pj = pn;
                 if (kk + TPA < ntot)
-                    pn = A.posf[row[list_slot(kk + TPA, nu, A.pmaxn)]];
+                    pn = A.posf[__ldcs(row + list_slot(kk + TPA, nu, A.pmaxn))];
                 float dx, dy, dz;
                 float const r2 = min_image_f(pi, pj, L, iL, dx, dy, dz);
                 if (r2 > T.fr_cut_sq)
@@ -299,14 +299,17 @@ __device__ __forceinline__ void force_row_mx(AtomsView const &A, TablesView cons
     if (sub >= n)
         return;
     auto slot = [&](int k) { return UPPER ? k : A.pmaxn - 1 - k; };
-    int jn = row[slot(sub)];
+    // the row's entries are read once per pass: streaming loads (evict first), so that
+    // they do not push the table and the partner records out of the L1 (measured: step
+    // 1.025 -> 0.987 ms at 16 x 13,500 atoms)
+    int jn = __ldcs(row + slot(sub));
     float4 pn = A.posf[jn];
     float2 fn = A.dF2f[jn];
     for (int kk = sub; kk < n; kk += TPA) {
         float4 const pj = pn;
         float2 const dFj2 = fn;
         if (kk + TPA < n) {
-            jn = row[slot(kk + TPA)];
+            jn = __ldcs(row + slot(kk + TPA));
             pn = A.posf[jn];
             fn = A.dF2f[jn];
         }
