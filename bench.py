@@ -494,7 +494,7 @@ def half_list_nbar(m, t, cell):
 # (the capture of the bench command at 4 replicas summarised under profiles/, the 200th
 # step, cold caches); the 16- and 32-replica entries scale it by the atoms processed. None
 # where not captured.
-_TRAFFIC_4 = 39.521536e6 + 0.017152e6
+_TRAFFIC_4 = 39.520000e6 + 0.023296e6
 TRAFFIC_PER_LAUNCH: dict = {("mixed", 4): _TRAFFIC_4, ("mixed", 16): 4 * _TRAFFIC_4,
                             ("mixed", 32): 8 * _TRAFFIC_4}
 
