@@ -99,6 +99,40 @@ def test_short_trajectory(ensemble):
         assert rel_err(th.eta, eo) < 1e-9 or np.max(np.abs(eo)) == 0
 
 
+@pytest.mark.parametrize("ensemble", [1, 2])
+def test_chain_beyond_series_range(ensemble):
+    """Chain momenta whose exponential arguments leave the branch-free series' range: the
+    top link of both chains at 4e15 1/s (x = dt p/Q up to 2.6, so every half step is redone
+    with the exact exponentials), the middle links at 2e14 1/s (x up to 0.13, inside the
+    range). 10 steps against the oracle, which takes the library exp throughout."""
+    import dataclasses
+    c = dynamics_case(nside=5, ensemble=ensemble)
+    T, q, p_eta, nf = c.thermo
+    q = np.asarray(q)
+    sign = np.where(np.arange(len(q)) % 2, 1.0, -1.0)
+    v = np.full(len(q), 2e14)
+    v[-1] = 4e15
+    p = np.asarray(p_eta, float).copy()
+    p[1:] = (sign * v * q)[1:]
+    Tb, qb, _, nfb = c.baro_thermo
+    qb = np.asarray(qb)
+    vb = np.full(len(qb), 2e14)
+    vb[-1] = 4e15
+    c = dataclasses.replace(c, thermo=(T, list(q), list(p), nf),
+                            baro_thermo=(Tb, list(qb), list(vb * qb), nfb))
+    o = oracle(c)
+    g = gpu(c)
+    for _ in range(10):
+        o.integrate()
+        g.integrate()
+    compare_state(g, o, 1e-9)
+    for which in (0, 1):
+        po, eo = o.chain(which)
+        th = g.thermostat if which == 0 else g.barostat.thermostat
+        assert rel_err(th.p_eta, po) < 1e-9
+        assert rel_err(th.eta, eo) < 1e-9
+
+
 def test_all_pairs_dynamics():
     """neighbors=False: every force call searches all pairs within the cutoff."""
     c = dynamics_case(nside=5, ensemble=1, neighbors=False, r_skin=1000.0)
