@@ -444,65 +444,88 @@ __global__ void k_reduce(AtomsView A) {
             (part[0][q] + part[1][q]) + (part[2][q] + part[3][q]);
 }
 
+// Row a and column b (a <= b) of entry q of the upper triangle of an n x n matrix stored
+// row by row.
+__device__ __forceinline__ void upper_pair(int q, int n, int &a, int &b) {
+    a = 0;
+    while (q >= n - a) {
+        q -= n - a;
+        ++a;
+    }
+    b = a + q;
+}
+
 // One sampled step: append what molecular_dynamics.py:1218-1238 reads to the replica's
 // ring, and, while accumulating, fold x = (sigma^B[6], N/V, V, etot_atom) and C^B into the
 // running means and co-moments (Welford's updates; the production-window sums behind
-// molecular_dynamics.py:776-958).
+// molecular_dynamics.py:776-958). Called by every thread of the block: each entry is one
+// thread's, with the same operations in the same order as a serial update.
 __device__ void record_sample(AtomsView const &A, int r, Replica *R, double V) {
+    __shared__ double s_d0[9], s_d1[9];
+    int const t = threadIdx.x;
     mdelast_observables const &o = R->obs;
-    if (A.ring && A.ring_cap > 0) {
+    bool const ring = A.ring && A.ring_cap > 0;
+    if (ring) {
         long const slot = static_cast<long>(R->n_samples) % A.ring_cap;
         mdelast_sample &s = A.ring[static_cast<size_t>(r) * A.ring_cap + slot];
-        s.time = o.time;
-        s.cycle = o.cycle;
-        s.temperature_kin = o.temperature_kin;
-        s.temperature_conf_inverse = o.temperature_conf_inverse;
-        s.total_laplacian = o.total_laplacian;
-        s.total_force2 = o.total_force2;
-        s.pressure = o.pressure;
-        for (int k = 0; k < 6; ++k) {
-            s.stress_tensor[k] = o.stress_tensor[k];
-            s.born_stress_tensor[k] = o.born_stress_tensor[k];
+        if (t == 0) {
+            s.time = o.time;
+            s.cycle = o.cycle;
+            s.temperature_kin = o.temperature_kin;
+            s.temperature_conf_inverse = o.temperature_conf_inverse;
+            s.total_laplacian = o.total_laplacian;
+            s.total_force2 = o.total_force2;
+            s.pressure = o.pressure;
+            s.etot_atom = o.etot_atom;
+            s.epot_atom = o.epot_atom;
+            s.epot_eam_atom = o.epot_eam_atom;
+            s.ekin_atom = o.ekin_atom;
+            s.etot_cons = o.etot_cons;
+            s.etot_cons_err = o.etot_cons_err;
+            s.volume = V;
+            s.status = static_cast<double>(o.status);
+        } else if (t >= 32 && t < 38) {
+            s.stress_tensor[t - 32] = o.stress_tensor[t - 32];
+            s.born_stress_tensor[t - 32] = o.born_stress_tensor[t - 32];
+        } else if (t >= 64 && t < 85) {
+            int a, b;
+            upper_pair(t - 64, 6, a, b);
+            s.born_elasticity_tensor[t - 64] = o.born_elasticity_tensor[6 * a + b];
         }
-        s.etot_atom = o.etot_atom;
-        s.epot_atom = o.epot_atom;
-        s.epot_eam_atom = o.epot_eam_atom;
-        s.ekin_atom = o.ekin_atom;
-        s.etot_cons = o.etot_cons;
-        s.etot_cons_err = o.etot_cons_err;
-        int q = 0;
-        for (int a = 0; a < 6; ++a)
-            for (int b = a; b < 6; ++b, ++q)
-                s.born_elasticity_tensor[q] = o.born_elasticity_tensor[6 * a + b];
-        s.volume = V;
-        s.status = static_cast<double>(o.status);
-        R->n_samples += 1.;
     }
-    if (!R->acc_on)
-        return;
+    bool const acc = R->acc_on;
     mdelast_fluct &f = R->acc;
-    double x[9];
-    for (int k = 0; k < 6; ++k)
-        x[k] = o.born_stress_tensor[k];
-    x[6] = R->n_atoms / V;
-    x[7] = V;
-    x[8] = o.etot_atom;
-    f.n += 1.;
-    double const inv_n = 1. / f.n;
-    double d0[9], d1[9];
-    for (int k = 0; k < 9; ++k) {
-        d0[k] = x[k] - f.mean[k];
-        f.mean[k] += d0[k] * inv_n;
-        d1[k] = x[k] - f.mean[k];
+    double const n1 = f.n + 1.;
+    double const inv_n = 1. / n1;
+    if (acc && t < 9) {
+        double const x = t < 6    ? o.born_stress_tensor[t]
+                         : t == 6 ? R->n_atoms / V
+                         : t == 7 ? V
+                                  : o.etot_atom;
+        double const d0 = x - f.mean[t];
+        double const m = f.mean[t] + d0 * inv_n;
+        s_d0[t] = d0;
+        s_d1[t] = x - m;
+        f.mean[t] = m;
     }
-    int q = 0;
-    for (int a = 0; a < 9; ++a)
-        for (int b = a; b < 9; ++b, ++q)
-            f.comoment[q] += d0[a] * d1[b];
-    q = 0;
-    for (int a = 0; a < 6; ++a)
-        for (int b = a; b < 6; ++b, ++q)
-            f.born_el_mean[q] += (o.born_elasticity_tensor[6 * a + b] - f.born_el_mean[q]) * inv_n;
+    __syncthreads();
+    if (t == 0) {
+        if (ring)
+            R->n_samples += 1.;
+        if (acc)
+            f.n = n1;
+    }
+    if (!acc)
+        return;
+    if (t < 45) {
+        int a, b;
+        upper_pair(t, 9, a, b);
+        f.comoment[t] += s_d0[a] * s_d1[b];
+    } else if (t >= 64 && t < 85) {
+        int a, b;
+        upper_pair(t - 64, 6, a, b);
+        f.born_el_mean[t - 64] += (o.born_elasticity_tensor[6 * a + b] - f.born_el_mean[t - 64]) * inv_n;
+    }
 }
 
 // what & 1: empty every replica's sample ring; what & 2: clear the fluctuation sums and
@@ -528,9 +551,8 @@ __global__ void k_samples_reset(AtomsView A, int what) {
     }
 }
 
-__device__ void thermodynamics(AtomsView const &A, Replica *R, int mode, int obs,
-                               const double *sf, const double *sd, double S, double ekin,
-                               double virial);
+__device__ void thermodynamics(Replica *R, int mode, int obs, const double *sf, const double *sd,
+                               double S, double ekin, double virial);
 
 __global__ void k_post(AtomsView A, int mode, int obs) {
     __shared__ Replica sR;
@@ -573,6 +595,15 @@ __global__ void k_post(AtomsView A, int mode, int obs) {
     int const ens = R->ensemble;
     double const dt = R->dt;
     mdelast_observables &o = R->obs;
+    // The box does not change in k_post: the volume of the thermodynamics (md_driver.cpp:
+    // 648-730), which divides the Born tensor, one entry per thread (zeros below the
+    // diagonal, as the reference stores it).
+    double const V = volume(R->h);
+    if (obs && t < 36) {
+        int const a = t / 6, b = t % 6;
+        o.born_elasticity_tensor[t] =
+            b < a ? 0. : (sf[F_CB + monomial_index(a, b)] + sd[D_CB + a * (11 - a) / 2 + b]) / V;
+    }
     if (t == 0) {
         double const virial = sf[F_VIRIAL] / -3.;
         s_virial = virial;
@@ -580,21 +611,8 @@ __global__ void k_post(AtomsView A, int mode, int obs) {
         double const vir_trace = -(sf[F_SIGMA] + sf[F_SIGMA + 1] + sf[F_SIGMA + 2]);
         if (fabs(virial / (vir_trace / 3.) - 1.) > 1e-7)
             atomicOr(&o.status, MDELAST_WARN_VIRIAL);
-        if (obs) {
-            double const lap = sf[F_LAP] + sd[D_LAP];
-            o.total_laplacian = lap;
-            int q = 0;
-            for (int a = 0; a < 6; ++a)
-                for (int b = 0; b < 6; ++b) {
-                    if (b < a) {
-                        o.born_elasticity_tensor[6 * a + b] = 0.;
-                        continue;
-                    }
-                    o.born_elasticity_tensor[6 * a + b] =
-                        sf[F_CB + monomial_index(a, b)] + sd[D_CB + q];
-                    ++q;
-                }
-        }
+        if (obs)
+            o.total_laplacian = sf[F_LAP] + sd[D_LAP];
         double ekin = sf[F_EKIN];
         if (mode == POST_STEP) {
             if (obs) {
@@ -625,13 +643,18 @@ __global__ void k_post(AtomsView A, int mode, int obs) {
     }
     __syncthreads();
     if (t == 0)
-        thermodynamics(A, R, mode, obs, sf, sd, s_S, s_ekin, s_virial);
+        thermodynamics(R, mode, obs, sf, sd, s_S, s_ekin, s_virial);
+    if (mode == POST_STEP && obs) {
+        __syncthreads();
+        record_sample(A, static_cast<int>(blockIdx.x), R, V);
+    }
     replica_store(&sR, A.rep + blockIdx.x);
 }
 
-// calculate_thermodynamics (md_driver.cpp:648-730) and the sample record, on the replica's
-// shared copy
-__device__ void thermodynamics(AtomsView const &A, Replica *R, int mode, int obs,
+// calculate_thermodynamics (md_driver.cpp:648-730) on the replica's shared copy, one thread;
+// k_post spreads the Born tensor's division by the volume and the sample record over the
+// block.
+__device__ void thermodynamics(Replica *R, int mode, int obs,
                                const double *sf, const double *sd, double S, double ekin,
                                double virial) {
     mdelast_observables &o = R->obs;
@@ -675,9 +698,6 @@ __device__ void thermodynamics(AtomsView const &A, Replica *R, int mode, int obs
         o.stress_tensor[k] = (-sf[F_SIGMA + k] + S2 * sf[F_MVV + k]) / V;
         o.born_stress_tensor[k] = sf[F_SIGMA + k] / V;
     }
-    if (obs)
-        for (int k = 0; k < 36; ++k)
-            o.born_elasticity_tensor[k] /= V;
     double const p_trace = o.stress_tensor[0] + o.stress_tensor[1] + o.stress_tensor[2];
     if (fabs(o.pressure / (p_trace / 3.) - 1.) > 1e-5)
         atomicOr(&o.status, MDELAST_FATAL_PRESSURE);
@@ -701,8 +721,6 @@ __device__ void thermodynamics(AtomsView const &A, Replica *R, int mode, int obs
     o.baro_epsilon = R->eps;
     o.baro_p_epsilon = R->p_eps;
     o.sample_observables = obs;
-    if (mode == POST_STEP && obs)
-        record_sample(A, static_cast<int>(blockIdx.x), R, V);
     R->sub_force = 0; // a forced pair-list refresh has run by now
 }
 
