@@ -700,14 +700,13 @@ __global__ void __launch_bounds__(kBlock) k_kick_drift(AtomsView A, TablesView T
 // FP64 min-image test on both atoms of a pair (so the list is symmetric), in list order.
 // A replica's rows are rebuilt when its list was rebuilt or when some atom has moved by
 // more than half the radius margin since the last refresh: then every pair now within
-// r_cut is still in the list. One warp per atom slot; the warp takes 32 entries at a time
-// and compacts the kept ones with a ballot.
+// r_cut is still in the list. One warp per atom slot at a time, grid-striding over the
+// slots; the warp takes 32 entries at a time and compacts the kept ones with a ballot. The
+// kernel runs every step and most steps refresh nothing: each block first asks whether any
+// replica is due (one flag per thread) and returns at once if none is, so a step without a
+// refresh costs one short wave instead of a warp per atom slot.
 
-__global__ void __launch_bounds__(256) k_sublist(AtomsView A) {
-    int const i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int const lane = threadIdx.x & 31;
-    if (i >= A.n_pad)
-        return;
+__device__ __forceinline__ void sublist_row(AtomsView const &A, int i, int lane) {
     int const r = A.rep_of[i];
     if (r < 0)
         return;
@@ -744,6 +743,20 @@ __global__ void __launch_bounds__(256) k_sublist(AtomsView A) {
         A.pn_dn[i] = kd;
         A.crd_ref[i] = make_double4(ci.x * hx, ci.y * hy, ci.z * hz, ci.w);
     }
+}
+
+__global__ void __launch_bounds__(256) k_sublist(AtomsView A) {
+    int due = 0;
+    for (int r = threadIdx.x; r < A.n_rep; r += blockDim.x) {
+        Replica const *R = A.rep + r;
+        due |= R->sub_force || R->sub_d2 > A.sub_half2;
+    }
+    if (!__syncthreads_or(due))
+        return;
+    int const lane = threadIdx.x & 31;
+    int const n_warps = gridDim.x * (blockDim.x >> 5);
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < A.n_pad; i += n_warps)
+        sublist_row(A, i, lane);
 }
 
 __global__ void k_sub_invalidate(AtomsView A) {

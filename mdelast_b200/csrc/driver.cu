@@ -65,6 +65,9 @@ int default_tpa(int n_atoms) {
 // atom group of kBlock/tpa atoms. Fills each replica's block range and the block ->
 // replica map; returns the grid size.
 constexpr int kTargetBlocks = 148 * 32;
+// k_sublist grid: one wave, 4 resident blocks of 256 threads (48 registers each) on each of
+// the 148 SMs
+constexpr int kSublistBlocks = 148 * 4;
 
 int deal_blocks(std::vector<Replica *> const &reps, int tpa, bool density,
                 std::vector<int> &blk_rep, int target = kTargetBlocks) {
@@ -153,7 +156,7 @@ struct mdelast_driver_s {
     void point_pair_list();
     void refresh_pair_list(cudaStream_t s) {
         if (A.crd_ref)
-            k_sublist<<<n_pad / 8, 256, 0, s>>>(A);
+            k_sublist<<<std::min(n_pad / 8, kSublistBlocks), 256, 0, s>>>(A);
     }
     double *d_pd = nullptr, *d_pf = nullptr, *d_red = nullptr;
     size_t cap_dmap = 0, cap_fmap = 0, cap_pd = 0, cap_pf = 0, cap_red = 0; // elements
