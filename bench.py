@@ -213,8 +213,7 @@ def run_ours(args, rank, world, local_rank):
         t1 = time.perf_counter()
         for s in range(e2e_steps):
             bb.run(1, REBUILD, 1, False)
-            for r in range(bb.n_replicas):
-                _ = bb.observables(r)
+            _ = bb.observables_all()
         t2 = time.perf_counter()
         for r in range(bb.n_replicas):
             _ = (bb.atoms(r, m.ATOM_POSITIONS), bb.atoms(r, m.ATOM_VELOCITIES))

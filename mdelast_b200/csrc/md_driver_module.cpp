@@ -629,6 +629,59 @@ py::dict obs_dict(mdelast_observables const &o) {
     return d;
 }
 
+// Every replica's observables in one dict of arrays with the replica as the first axis
+// (the fields of obs_dict).
+py::dict obs_dict_all(std::vector<mdelast_observables> const &o) {
+    size_t const n = o.size();
+    py::dict d;
+    auto col = [&](char const *name, double mdelast_observables::*f) {
+        py::array_t<double> a(n);
+        for (size_t i = 0; i < n; ++i)
+            a.mutable_data()[i] = o[i].*f;
+        d[name] = a;
+    };
+    col("epot_eam_atom", &mdelast_observables::epot_eam_atom);
+    col("epot_atom", &mdelast_observables::epot_atom);
+    col("ekin_atom", &mdelast_observables::ekin_atom);
+    col("etot_atom", &mdelast_observables::etot_atom);
+    col("etot_cons", &mdelast_observables::etot_cons);
+    col("etot_cons_err", &mdelast_observables::etot_cons_err);
+    col("virial", &mdelast_observables::virial);
+    col("total_laplacian", &mdelast_observables::total_laplacian);
+    col("total_force2", &mdelast_observables::total_force2);
+    col("temperature_kin", &mdelast_observables::temperature_kin);
+    col("temperature_conf_inverse", &mdelast_observables::temperature_conf_inverse);
+    col("pressure", &mdelast_observables::pressure);
+    col("time", &mdelast_observables::time);
+    col("baro_epsilon", &mdelast_observables::baro_epsilon);
+    col("baro_p_epsilon", &mdelast_observables::baro_p_epsilon);
+    py::array_t<unsigned long long> cyc(n);
+    py::array_t<uint32_t> status(n);
+    py::array_t<double> vol(n), bs({n, size_t(6)}), st({n, size_t(6)}), box({n, size_t(3)}),
+        cb({n, size_t(6), size_t(6)});
+    for (size_t i = 0; i < n; ++i) {
+        cyc.mutable_data()[i] = static_cast<unsigned long long>(o[i].cycle);
+        status.mutable_data()[i] = o[i].status;
+        vol.mutable_data()[i] = o[i].box[0] * (o[i].box[4] * o[i].box[8]);
+        for (int k = 0; k < 3; ++k)
+            box.mutable_data()[3 * i + k] = o[i].box[4 * k];
+        for (int k = 0; k < 6; ++k) {
+            bs.mutable_data()[6 * i + k] = o[i].born_stress_tensor[k];
+            st.mutable_data()[6 * i + k] = o[i].stress_tensor[k];
+        }
+        std::copy(o[i].born_elasticity_tensor, o[i].born_elasticity_tensor + 36,
+                  cb.mutable_data() + 36 * i);
+    }
+    d["cycle"] = cyc;
+    d["born_stress_tensor"] = bs;
+    d["stress_tensor"] = st;
+    d["born_elasticity_tensor"] = cb;
+    d["volume"] = vol;
+    d["box"] = box;
+    d["status"] = status;
+    return d;
+}
+
 // Many independent replicas sharing one potential, advanced together on one GPU (new in
 // this implementation; the reference runs replicas as separate processes). Per replica:
 // positions (N,3) and velocities (N,3) arrays [cgs], types, ensemble, thermostat and
@@ -741,6 +794,12 @@ class BatchedMDDriver {
         mdelast_observables o;
         check(mdelast_batch_get_observables(d_, r, &o));
         return obs_dict(o);
+    }
+    py::dict observables_all() {
+        std::vector<mdelast_observables> o(static_cast<size_t>(n_replicas()));
+        for (int r = 0; r < n_replicas(); ++r)
+            check(mdelast_batch_get_observables(d_, r, &o[static_cast<size_t>(r)]));
+        return obs_dict_all(o);
     }
     py::array_t<uint32_t> status() {
         py::array_t<uint32_t> a(static_cast<size_t>(n_replicas()));
@@ -1018,6 +1077,7 @@ PYBIND11_MODULE(md_driver_module, m) {
         .def("calculate_neighbors", &BatchedMDDriver::calculate_neighbors)
         .def_property("sample_observables", &BatchedMDDriver::get_sample, &BatchedMDDriver::set_sample)
         .def("observables", &BatchedMDDriver::observables, py::arg("replica"))
+        .def("observables_all", &BatchedMDDriver::observables_all)
         .def("status", &BatchedMDDriver::status)
         .def("atoms", &BatchedMDDriver::atoms, py::arg("replica"), py::arg("field"))
         .def("neighbor_list", &BatchedMDDriver::neighbor_list, py::arg("replica"))

@@ -66,3 +66,13 @@ def test_batch_uneven_sizes_mixed_precision():
         o = b.observables(r)
         assert o["status"] & 0xff == 0
         assert abs(o["etot_cons"] / e0[r] - 1.0) < 5e-5, (r, cells[r].T)
+    # the batch-wide readout holds the same values, replica along the first axis
+    allo = b.observables_all()
+    for r in range(b.n_replicas):
+        o = b.observables(r)
+        for k in ("etot_cons", "pressure", "temperature_kin", "time", "volume", "cycle",
+                  "status"):
+            assert allo[k][r] == o[k], k
+        for k in ("stress_tensor", "born_stress_tensor", "born_elasticity_tensor"):
+            assert np.array_equal(allo[k][r], np.asarray(o[k])), k
+        assert tuple(allo["box"][r]) == tuple(o["box"])
