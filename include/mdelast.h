@@ -66,6 +66,10 @@ const char *mdelast_last_error(void);
 int mdelast_abi_version(void);
 /* 1 when a CUDA device is usable, 0 otherwise (no error). */
 int mdelast_device_available(void);
+/* Drivers take their device buffers from the device's default stream-ordered memory pool,
+ * which keeps freed memory for the next driver; this hands the unused part of it back to
+ * the device. No reference counterpart (the reference holds host memory only). */
+int mdelast_release_cached_memory(int32_t device);
 
 /* ---------------------------------------------------------------------------------
  * Tabulated functions.

@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "host_tables.h"
@@ -28,15 +29,49 @@ using namespace mdelast;
 
 namespace {
 
-template <typename T> int dalloc(T **p, size_t n) {
-    CK(cudaMalloc(reinterpret_cast<void **>(p), sizeof(T) * (n > 0 ? n : 1)));
-    CK(cudaMemset(*p, 0, sizeof(T) * (n > 0 ? n : 1)));
+// Device buffers come from the device's default stream-ordered memory pool, whose release
+// threshold is raised once per device so that the process keeps freed memory: a driver
+// created after another was destroyed (the NPT and NVT stages of a protocol, a warm start's
+// corrected boxes) reuses its pages instead of mapping new ones.
+// mdelast_release_cached_memory() hands the unused part back to the device.
+int keep_pool(int dev) {
+    static std::mutex mu;
+    static std::vector<char> done;
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev < 0)
+        return MDELAST_OK;
+    if (done.size() <= static_cast<size_t>(dev))
+        done.resize(static_cast<size_t>(dev) + 1, 0);
+    if (done[static_cast<size_t>(dev)])
+        return MDELAST_OK;
+    cudaMemPool_t pool;
+    CK(cudaDeviceGetDefaultMemPool(&pool, dev));
+    uint64_t keep = UINT64_MAX;
+    CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    done[static_cast<size_t>(dev)] = 1;
     return MDELAST_OK;
 }
 
+// Allocated, zeroed and complete on return (the driver's own stream does not order against
+// the legacy stream the pool is used on).
+template <typename T> int dalloc(T **p, size_t n) {
+    size_t const bytes = sizeof(T) * (n > 0 ? n : 1);
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (int rc = keep_pool(dev))
+        return rc;
+    CK(cudaMallocAsync(reinterpret_cast<void **>(p), bytes, cudaStreamLegacy));
+    CK(cudaMemsetAsync(*p, 0, bytes, cudaStreamLegacy));
+    CK(cudaStreamSynchronize(cudaStreamLegacy));
+    return MDELAST_OK;
+}
+
+// Returned to the pool once all work on the device has finished, as cudaFree would wait.
 template <typename T> void dfree(T *&p) {
-    if (p)
-        cudaFree(p);
+    if (p) {
+        cudaDeviceSynchronize();
+        cudaFreeAsync(p, cudaStreamLegacy);
+    }
     p = nullptr;
 }
 
@@ -682,6 +717,20 @@ int mdelast_driver_s::check_status() {
 }
 
 extern "C" {
+
+int mdelast_release_cached_memory(int32_t device) {
+    clear_error();
+    int n = 0;
+    CK(cudaGetDeviceCount(&n));
+    if (device < 0 || device >= n)
+        return fail(MDELAST_ERR_ARGUMENT, "device %d out of range", device);
+    CK(cudaSetDevice(device));
+    CK(cudaDeviceSynchronize());
+    cudaMemPool_t pool;
+    CK(cudaDeviceGetDefaultMemPool(&pool, device));
+    CK(cudaMemPoolTrimTo(pool, 0));
+    return MDELAST_OK;
+}
 
 int mdelast_device_available(void) {
     int n = 0;

@@ -1160,6 +1160,8 @@ PYBIND11_MODULE(md_driver_module, m) {
     units.attr("fs") = 1e-15;
 
     m.def("device_available", []() { return mdelast_device_available() != 0; });
+    m.def("release_cached_memory", [](int device) { check(mdelast_release_cached_memory(device)); },
+          py::arg("device") = 0);
     m.def("set_default_precision", [](std::string const &p) {
         if (p != "fp64" && p != "mixed")
             throw py::value_error("precision must be 'fp64' or 'mixed'");

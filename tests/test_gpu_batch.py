@@ -76,3 +76,25 @@ def test_batch_uneven_sizes_mixed_precision():
         for k in ("stress_tensor", "born_stress_tensor", "born_elasticity_tensor"):
             assert np.array_equal(allo[k][r], np.asarray(o[k])), k
         assert tuple(allo["box"][r]) == tuple(o["box"])
+
+
+def test_memory_reused_and_released():
+    """A batch created in the memory its predecessor freed (kept by the device's pool)
+    gives the same results as the first, and again after the pool was handed back."""
+    import md_driver_module as m
+    from mdelast_b200.systems import cuzn_cell, make_batch
+    t = tables()
+    cells = [cuzn_cell(t, 5, n_zn=30, velocity_seed=s) for s in (0, 1)]
+
+    def run():
+        b = make_batch(m, t, cells, precision="mixed")
+        b.run(30, 20, 1)
+        out = [(b.observables(r)["etot_cons"], b.observables(r)["pressure"])
+               for r in range(b.n_replicas)]
+        del b
+        return out
+
+    first = run()
+    assert run() == first
+    m.release_cached_memory(0)
+    assert run() == first
