@@ -117,6 +117,10 @@ def test_no_device_no_fallback(lib):
     from helpers import gpu, static_case
     with pytest.raises(RuntimeError, match="no CUDA device"):
         gpu(static_case())
+    # the memory-pool release has nothing to release and says why
+    assert lib.mdelast_release_cached_memory(0) != 0
+    with pytest.raises(RuntimeError):
+        m.release_cached_memory(0)
 
 
 def test_bspline_table_matches_oracle(lib):
