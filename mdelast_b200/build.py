@@ -3,7 +3,11 @@
 * ``libmdelast_cuda.so``: the CUDA kernels and the C-ABI of ``include/mdelast.h``,
   compiled for sm_100a only;
 * ``md_driver_module<ext>.so``: the pybind11 module that mirrors the reference's
-  ``md_driver_module`` on top of that C-ABI.
+  ``md_driver_module`` on top of that C-ABI;
+* ``data/potentials/``: the potential files of an mdelast checkout, when one is found
+  (``$MDELAST_REFERENCE``, else a checkout called ``reference`` beside this repository).
+  Their licences keep them out of this repository's history; the directory is ignored by
+  git and read by ``mdelast_b200.potentials.find_potential``.
 
 Run ``python -m mdelast_b200.build``. Nothing here needs a GPU.
 """
@@ -11,6 +15,7 @@ Run ``python -m mdelast_b200.build``. Nothing here needs a GPU.
 from __future__ import annotations
 
 import os
+import shutil
 import subprocess
 import sys
 import sysconfig
@@ -83,9 +88,38 @@ def build_python_module():
     return out
 
 
+def reference_checkout():
+    """The mdelast checkout next to this repository, or None."""
+    for c in (os.environ.get("MDELAST_REFERENCE"), os.path.join(os.path.dirname(ROOT), "reference")):
+        if c and os.path.isdir(os.path.join(c, "potentials")):
+            return os.path.abspath(c)
+    return None
+
+
+def stage_potentials():
+    """Copy the checkout's potential files into ``data/potentials`` (unchanged files are
+    left alone). Returns the number of files staged."""
+    ref = reference_checkout()
+    if ref is None:
+        return 0
+    src_dir = os.path.join(ref, "potentials")
+    dst_dir = os.path.join(HERE, "data", "potentials")
+    os.makedirs(dst_dir, exist_ok=True)
+    n = 0
+    for name in sorted(os.listdir(src_dir)):
+        if not name.endswith((".eam.alloy", ".eam.alloy.txt", ".eam.fs.txt")):
+            continue
+        src, dst = os.path.join(src_dir, name), os.path.join(dst_dir, name)
+        if _stale(dst, [src]) or os.path.getsize(dst) != os.path.getsize(src):
+            shutil.copyfile(src, dst)
+        n += 1
+    return n
+
+
 def build_all(verbose_ptxas=False):
     lib = build_cuda_library(verbose_ptxas=verbose_ptxas)
     mod = build_python_module() if os.path.exists(os.path.join(CSRC, "md_driver_module.cpp")) else None
+    stage_potentials()
     return lib, mod
 
 

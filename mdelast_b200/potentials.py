@@ -1,22 +1,23 @@
-"""Readers for LAMMPS SETFL embedded-atom potential files.
+"""Readers for LAMMPS SETFL (and single-element Finnis-Sinclair) EAM potential files.
 
-They restate the node-array construction of mdelast's loader
-(``src/python/get_potential.py:58-147`` for multi-element ``*.eam.alloy`` files and
-``:150-257`` for the single-element ``*.eam.alloy.txt`` form). Each numpy/scipy
-operation and its argument units are the same, so the node arrays handed to the
-tables are bit-identical to the ones the reference builds its ``TablePotential`` and
-``EAM`` objects from:
+One tokenizer (:func:`_parse_setfl`) reads the layout, with values one or several to a
+line. Two unit conversions then follow the two loaders of mdelast, because their
+operation orders differ and the node arrays must be the reference's bit for bit:
 
-* values are converted to CGS exactly as the reference does (``Units.ev``,
-  ``Units.angstrom``);
-* node derivatives come from ``scipy.interpolate.UnivariateSpline(k=5, s=0)``
-  (``get_potential.py:49-55``);
-* pair blocks are read in SETFL order 11, 21, 22, 31, ... into slot
-  ``j(j+1)/2 + i`` (``get_potential.py:122-145``), and ``phi = (r phi)/r`` with
-  ``phi[0] = phi[1]``.
+* :func:`read_eam_alloy`: the alloy loader (``src/python/get_potential.py:58-147``),
+  grids built in cgs, ``phi = (r phi) / r_cm * eV * angstrom``;
+* :func:`read_eam_single`: the single-element loader (``get_potential.py:150-257``) of
+  the pure-Cu example, grids built in angstrom, ``phi = (r phi) / r_A * eV``, then the
+  grids and densities converted to cgs; ``*.eam.fs.txt`` files get the core-fill
+  replacement of that loader.
 
-The reader returns plain arrays (:class:`SetflTables`). :func:`make_objects` turns
-them into the ``TablePotential``/``EAM`` objects of a ``md_driver_module``.
+Node derivatives come from ``scipy.interpolate.UnivariateSpline(k=5, s=0)``
+(``get_potential.py:49-55``); pair blocks go to slot ``j(j+1)/2 + i``
+(``get_potential.py:122-145``) and ``phi[0] = phi[1]``. ``tests/test_readers.py`` checks
+every array against digests of the reference loader's output.
+
+The readers return plain arrays (:class:`SetflTables`). :func:`make_objects` turns them
+into the ``TablePotential``/``EAM`` objects of a ``md_driver_module``.
 """
 
 from __future__ import annotations
@@ -79,152 +80,192 @@ class SetflTables:
         return [e[2] / Units.Navogadro for e in self.elements]
 
 
-def _tokens(lines, start):
-    """Yield (line_index, token) for whitespace tokens from line ``start`` on."""
-    for li in range(start, len(lines)):
-        for tok in lines[li].split():
-            yield li, tok
+@dataclass
+class _SetflText:
+    """The numbers of one SETFL (or single-element Finnis-Sinclair) file, in file units:
+    eV, angstrom, r*phi in eV angstrom. ``pair_rphi`` keeps the file's block order."""
+
+    elements: list         # [symbol, Z, atomic weight, lattice constant (angstrom)]
+    n_rho: int
+    d_rho: float
+    n_r: int
+    d_r: float
+    embed: list            # F(rho) per element
+    density: list          # rho(r) per element
+    pair_rphi: list        # r * phi(r), blocks 11, 21, 22, 31, ...
+
+
+class _NumberStream:
+    """Numbers of a text file read one after the other across line boundaries, with the
+    line-level access that element header lines need."""
+
+    def __init__(self, lines, first_line):
+        self._lines = lines
+        self._li = first_line
+        self._pending = []
+
+    def header_line(self):
+        if self._pending:
+            raise ValueError(f"element header expected at a line start (line {self._li})")
+        line = self._lines[self._li].split()
+        self._li += 1
+        return line
+
+    def take(self, count):
+        out = np.empty(count)
+        k = 0
+        while k < count:
+            if not self._pending:
+                if self._li >= len(self._lines):
+                    raise ValueError(f"file ends {count - k} numbers short of a block")
+                self._pending = self._lines[self._li].split()[::-1]
+                self._li += 1
+                continue
+            out[k] = float(self._pending.pop())
+            k += 1
+        return out
+
+
+def _parse_setfl(path) -> _SetflText:
+    """Parse the LAMMPS ``setfl`` layout: three comment lines, the element line, the grid
+    line ``Nrho drho Nr dr rcut``, then per element a header ``Z mass a lattice`` followed by
+    F(rho) and rho(r), then the pair blocks r*phi(r). Values may sit one or several to a
+    line; blocks need not start on a new line."""
+    with open(path) as fh:
+        lines = fh.readlines()
+    head = lines[3].split()
+    n_el = int(head[0])
+    symbols = head[1:1 + n_el]
+    grid = lines[4].split()
+    n_rho, n_r = int(grid[0]), int(grid[2])
+    d_rho, d_r = float(grid[1]), float(grid[3])
+    stream = _NumberStream(lines, 5)
+    elements, embed, density = [], [], []
+    for sym in symbols:
+        z, weight, a0 = (float(x) for x in stream.header_line()[:3])
+        elements.append([sym, z, weight, a0])
+        embed.append(stream.take(n_rho))
+        density.append(stream.take(n_r))
+    pair = [stream.take(n_r) for _ in range(n_el * (n_el + 1) // 2)]
+    return _SetflText(elements, n_rho, d_rho, n_r, d_r, embed, density, pair)
+
+
+def _pair_slot_order(n_el):
+    """Slot ``j(j+1)/2 + i`` of each file block (blocks run 11, 21, 22, 31, 32, 33, ...,
+    i.e. (i, j) with i <= j and j the outer index; ``md_driver.cpp:341-343``)."""
+    return [j * (j + 1) // 2 + i for j in range(n_el) for i in range(j + 1)]
+
+
+FS_FILL = 1e12       # placeholder the Mendelev Cu2 FS file uses inside the core region
+
+
+def _fill_core(values):
+    """Finnis-Sinclair tables of the Mendelev Cu file fill the innermost nodes of rho(r)
+    and r*phi(r) with 1e12; the reference replaces that run by the first real value
+    (``get_potential.py:186-211``, where the run is the first 167 nodes)."""
+    n = 0
+    while n < len(values) and values[n] == FS_FILL:
+        n += 1
+    if 0 < n < len(values):
+        values[:n] = values[n]
+    return values
 
 
 def read_eam_alloy(path) -> SetflTables:
-    """Multi-element SETFL reader (``get_potential.py:58-147``)."""
-    with open(path, "r") as f:
-        lines = f.readlines()
-    header_lines = 3
-    element_info = lines[header_lines].split()
-    num_elements = int(element_info[0])
-    elements = [[element_info[i]] for i in range(1, num_elements + 1)]
-    param_line = lines[header_lines + 1].split()
-    Nrho = int(param_line[0])
-    drho = float(param_line[1]) / Units.angstrom**3
-    Nr = int(param_line[2])
-    dr = float(param_line[3]) * Units.angstrom
-    r_grid = np.linspace(0.0, dr * (Nr - 1.0), Nr)  # cm
-    rho_grid = np.linspace(0.0, drho * (Nrho - 1.0), Nrho)
-
-    # The file is a sequence of numbers after each element's header line. Collect the
-    # numeric blocks line-wise so that one or several values per line both work.
-    index = 5
-    F_all, dF_all, d2F_all, rho_all, drho_all, d2rho_all = [], [], [], [], [], []
-    for i in range(num_elements):
-        atomic_number, atomic_weight, a_lattice = [
-            float(s) for s in lines[index].split("\n")[0].split()[:-1]
-        ]
-        elements[i].extend([atomic_number, atomic_weight, a_lattice])
-        index += 1
-        vals, index = _read_numbers(lines, index, Nrho + Nr)
-        F = np.array(vals[:Nrho]) * Units.ev
-        rho = np.array(vals[Nrho:Nrho + Nr]) / Units.angstrom**3
-        drhodr, d2rhodr2 = get_derivatives(x=r_grid, y=rho)
-        dFdrho, d2Fdrho = get_derivatives(x=rho_grid, y=F)
-        F_all.append(F); dF_all.append(dFdrho); d2F_all.append(d2Fdrho)
-        rho_all.append(rho); drho_all.append(drhodr); d2rho_all.append(d2rhodr2)
-    npot = num_elements * (num_elements + 1) // 2
-    phi_all = [None] * npot
-    dphi_all = [None] * npot
-    d2phi_all = [None] * npot
-    i, j = 0, 0
+    """Multi-element SETFL potential with the unit conversions of the reference's alloy
+    loader (``get_potential.py:58-147``): the grids are built in cgs, r*phi is divided by
+    the cgs radius and scaled by eV and angstrom afterwards."""
+    f = _parse_setfl(path)
+    A3 = Units.angstrom**3
+    drho = f.d_rho / A3
+    dr = f.d_r * Units.angstrom
+    r_grid = np.linspace(0.0, dr * (f.n_r - 1.0), f.n_r)
+    rho_grid = np.linspace(0.0, drho * (f.n_rho - 1.0), f.n_rho)
+    embed = [F * Units.ev for F in f.embed]
+    dens = [rho / A3 for rho in f.density]
+    d_dens = [get_derivatives(x=r_grid, y=rho) for rho in dens]
+    d_embed = [get_derivatives(x=rho_grid, y=F) for F in embed]
+    n_pot = len(f.pair_rphi)
+    phi_s, dphi_s, d2phi_s = [None] * n_pot, [None] * n_pot, [None] * n_pot
     with np.errstate(divide="ignore", invalid="ignore"):
-        for _ in range(npot):
-            pot_index = j * (j + 1) // 2 + i
-            vals, index = _read_numbers(lines, index, Nr)
-            phir = np.array(vals)
-            phi = phir / r_grid * Units.ev * Units.angstrom
+        for slot, rphi in zip(_pair_slot_order(len(f.elements)), f.pair_rphi):
+            phi = rphi / r_grid * Units.ev * Units.angstrom
             phi[0] = phi[1]
-            dphidr, d2phidr2 = get_derivatives(x=r_grid, y=phi)
-            phi_all[pot_index], dphi_all[pot_index], d2phi_all[pot_index] = phi, dphidr, d2phidr2
-            if i == j:
-                j += 1
-                i = 0
-            else:
-                i += 1
+            phi_s[slot] = phi
+            dphi_s[slot], d2phi_s[slot] = get_derivatives(x=r_grid, y=phi)
     return SetflTables(
-        elements=elements, n_r=Nr, dr=dr, n_rho=Nrho, drho=drho,
+        elements=f.elements, n_r=f.n_r, dr=dr, n_rho=f.n_rho, drho=drho,
         rcut=float(r_grid[-1]), rhomax=float(rho_grid[-1]),
         rmin_fatal=1e-2 * Units.angstrom,
-        phi=np.array(phi_all), dphi=np.array(dphi_all), d2phi=np.array(d2phi_all),
-        rho=np.array(rho_all), drho_dr=np.array(drho_all), d2rho_dr2=np.array(d2rho_all),
-        F=np.array(F_all), dF=np.array(dF_all), d2F=np.array(d2F_all),
+        phi=np.array(phi_s), dphi=np.array(dphi_s), d2phi=np.array(d2phi_s),
+        rho=np.array(dens), drho_dr=np.array([d[0] for d in d_dens]),
+        d2rho_dr2=np.array([d[1] for d in d_dens]),
+        F=np.array(embed), dF=np.array([d[0] for d in d_embed]),
+        d2F=np.array([d[1] for d in d_embed]),
         source=str(path),
     )
 
 
-def _read_numbers(lines, index, count):
-    """Read ``count`` numbers starting at line ``index``; return (values, next line)."""
-    vals = []
-    li = index
-    while len(vals) < count:
-        toks = lines[li].split()
-        vals.extend(float(t) for t in toks)
-        li += 1
-    if len(vals) != count:
-        raise ValueError(f"SETFL block at line {index + 1}: expected {count} values, "
-                         f"a line boundary falls inside the block")
-    return vals, li
-
-
 def read_eam_single(path, a_factor=1.0) -> SetflTables:
-    """Single-element ``*.eam.alloy.txt`` reader (``get_potential.py:150-257``), the
-    loader of the pure-Cu example. Units follow that function: the r grid is built in
-    angstrom and scaled to cm afterwards."""
-    with open(path, "r") as f:
-        all_lines = f.readlines()
-    line = all_lines[5].split("\n")[0].split()[:-1]
-    atomic_number, atomic_weight, a_lattice = [float(s) for s in line]
-    params = np.loadtxt(path, skiprows=4, max_rows=1)[:]
-    Nrho, drho, Nr, dr, rcut = params
-    Nrho = int(Nrho)
-    Nr = int(Nr)
-    r_grid = np.linspace(0.0, dr * (Nr - 1.0), Nr)  # angstrom
-    rho_grid = np.linspace(0.0, drho * (Nrho - 1.0), Nrho)  # angstrom**-3
-    data = np.loadtxt(path, skiprows=6)
-    if not (len(data.shape) == 1 and data.shape[0] == Nrho + Nr + Nr):
-        raise ValueError("unsupported single-element SETFL layout")
-    F = data[:Nrho]
-    rho = data[Nrho:Nrho + Nr]
-    phir = data[Nrho + Nr:]
-    F *= Units.ev
+    """Single-element potential (``*.eam.alloy.txt`` setfl or ``*.eam.fs.txt``
+    Finnis-Sinclair) with the unit conversions of the reference's single-element loader
+    (``get_potential.py:150-257``, the loader of the pure-Cu example): the grids are built in
+    angstrom, r*phi is divided by the angstrom radius and scaled by eV, and the grids and
+    densities are converted to cgs afterwards. ``meta["a_lattice"]`` is the file's lattice
+    constant times ``a_factor`` in cm, as that loader hands it to ``Material``."""
+    f = _parse_setfl(path)
+    if len(f.elements) != 1:
+        raise ValueError(f"{path}: single-element loader given {len(f.elements)} elements")
+    rho_r, rphi = f.density[0], f.pair_rphi[0]
+    if str(path).endswith("eam.fs.txt"):
+        rho_r, rphi = _fill_core(rho_r.copy()), _fill_core(rphi.copy())
+    r_ang = np.linspace(0.0, f.d_r * (f.n_r - 1.0), f.n_r)
+    rho_grid_ang = np.linspace(0.0, f.d_rho * (f.n_rho - 1.0), f.n_rho)
+    F = f.embed[0] * Units.ev
     with np.errstate(divide="ignore", invalid="ignore"):
-        phi = phir / r_grid * Units.ev
+        phi = rphi / r_ang * Units.ev
     phi[0] = phi[1]
-    dr *= Units.angstrom
-    rcut *= Units.angstrom
-    r_grid *= Units.angstrom
-    drho /= Units.angstrom**3
-    rho /= Units.angstrom**3
-    rho_grid /= Units.angstrom**3
-    dphidr, d2phidr2 = get_derivatives(x=r_grid, y=phi)
-    drhodr, d2rhodr2 = get_derivatives(x=r_grid, y=rho)
-    dFdrho, d2Fdrho = get_derivatives(x=rho_grid, y=F)
+    A3 = Units.angstrom**3
+    r_grid = r_ang * Units.angstrom
+    rho = rho_r / A3
+    rho_grid = rho_grid_ang / A3
+    dphi, d2phi = get_derivatives(x=r_grid, y=phi)
+    drho_dr, d2rho_dr2 = get_derivatives(x=r_grid, y=rho)
+    dF, d2F = get_derivatives(x=rho_grid, y=F)
+    el = f.elements[0]
     return SetflTables(
-        elements=[["Cu", atomic_number, atomic_weight, a_lattice]],
-        n_r=Nr, dr=float(dr), n_rho=Nrho, drho=float(drho),
-        rcut=float(r_grid[-1]), rhomax=float(rho_grid[-1]),
+        elements=[list(el)], n_r=f.n_r, dr=f.d_r * Units.angstrom, n_rho=f.n_rho,
+        drho=f.d_rho / A3, rcut=float(r_grid[-1]), rhomax=float(rho_grid[-1]),
         rmin_fatal=1e-2 * Units.angstrom,
-        phi=phi[None, :], dphi=dphidr[None, :], d2phi=d2phidr2[None, :],
-        rho=rho[None, :], drho_dr=drhodr[None, :], d2rho_dr2=d2rhodr2[None, :],
-        F=F[None, :], dF=dFdrho[None, :], d2F=d2Fdrho[None, :],
-        source=str(path), meta={"a_lattice": a_lattice * Units.angstrom * a_factor},
+        phi=phi[None, :], dphi=dphi[None, :], d2phi=d2phi[None, :],
+        rho=rho[None, :], drho_dr=drho_dr[None, :], d2rho_dr2=d2rho_dr2[None, :],
+        F=F[None, :], dF=dF[None, :], d2F=d2F[None, :],
+        source=str(path), meta={"a_lattice": el[3] * Units.angstrom * a_factor},
     )
 
 
 def read_setfl(path) -> SetflTables:
-    """Dispatch on the file name as the reference's two loaders are used:
-    ``*.eam.alloy.txt`` single-element form, otherwise the multi-element reader."""
-    if str(path).endswith("eam.alloy.txt"):
+    """Pick the loader by file name as the reference's scripts do: the single-element
+    loader for ``*.eam.alloy.txt`` and ``*.eam.fs.txt``, the alloy loader otherwise."""
+    if str(path).endswith(("eam.alloy.txt", "eam.fs.txt")):
         return read_eam_single(path)
     return read_eam_alloy(path)
 
 
+PACKAGE_POTENTIALS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data",
+                                  "potentials")
+
+
 def find_potential(name: str):
-    """Locate a potential file by name: ``$MDELAST_POTENTIALS``, then the copy the oracle
-    build recipe places in ``oracle/_ref/potentials``. Returns None when absent."""
-    here = os.path.dirname(os.path.abspath(__file__))
+    """Locate a potential file by name: ``$MDELAST_POTENTIALS`` first, then the package's
+    ``data/potentials`` directory (filled by ``mdelast_b200.build`` from an mdelast
+    checkout; the files' licences keep them out of this repository's history). Returns
+    None when absent."""
     cands = []
     env = os.environ.get("MDELAST_POTENTIALS")
     if env:
         cands.append(os.path.join(env, name))
-    cands.append(os.path.join(here, "..", "oracle", "_ref", "potentials", name))
+    cands.append(os.path.join(PACKAGE_POTENTIALS, name))
     for c in cands:
         if os.path.isfile(c):
             return os.path.abspath(c)

@@ -4,18 +4,21 @@ files (benchmarks/expected/zn06_300K.json and l12_cuzn3_5K.json): Z1, Cu-6 at.% 
 300 K, and L1, L1_2 CuZn3 at 5 K, each an NPT stage then an NVT stage of 50,000 + 100,000
 steps. Per quantity it keeps the check itself ("expected" with "tol", or the one-sided
 "max" / "min", or "info" for report-only values), the unit, and the reference run's own
-standard error and velocity-replica spread where given. The reference checkout is read
-from REFERENCE (default /root/reference)."""
+standard error and velocity-replica spread where given. The reference checkout is
+``$MDELAST_REFERENCE`` or a checkout called ``reference`` beside this repository."""
 
 import json
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("REFERENCE", "/root/reference")
 KEEP = ("expected", "tol", "max", "min", "info", "unit", "se_run", "s_vel")
 
 
 def main():
+    import sys
+    sys.path.insert(0, HERE)
+    from refroot import reference_root
+    REF = reference_root(sys.argv[1] if len(sys.argv) > 1 else None)
     out = {}
     for name in ("zn06_300K", "l12_cuzn3_5K"):
         d = json.load(open(os.path.join(REF, "benchmarks", "expected", name + ".json")))

@@ -18,7 +18,9 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    sys.path.insert(0, HERE)
+    from refroot import reference_root
+    ref = reference_root(sys.argv[1] if len(sys.argv) > 1 else None)
     sys.modules.setdefault("h5py", types.ModuleType("h5py"))
     sys.path[:0] = [os.path.join(ref, "src", "python"), os.path.join(ROOT, "mdelast_b200", "lib")]
     import md_driver_module as m

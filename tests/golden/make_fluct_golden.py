@@ -116,7 +116,9 @@ def run_reference(ref_py, ensemble, s, N, V0, T, P, n_therm):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    sys.path.insert(0, HERE)
+    from refroot import reference_root
+    ref = reference_root(sys.argv[1] if len(sys.argv) > 1 else None)
     ref_py = os.path.join(ref, "src", "python")
     N, T, P = 13500, 300.0, 1e-10 * 1e10
     V0 = N / 4 * (3.6345e-8) ** 3

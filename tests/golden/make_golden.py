@@ -1,8 +1,9 @@
 """Regenerate the golden fixtures of this directory from mdelast's own test data.
 
-Run in a container where the mdelast sources are mounted (default /root/reference):
+Run where an mdelast checkout is available (``--ref``, else ``$MDELAST_REFERENCE``, else a
+checkout called ``reference`` beside this repository):
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py [--ref PATH]
 
 Writes
 * ``smoke_static.json``: benchmark S Part A6 expected values per table interpolation
@@ -38,8 +39,10 @@ def read_lammps_data(path):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=None)
     a = ap.parse_args()
+    from refroot import reference_root
+    a.ref = reference_root(a.ref)
     smoke = json.load(open(os.path.join(a.ref, "benchmarks", "expected", "smoke.json")))
     checks = smoke["checks"]
     out = {"source": "mdelast benchmarks/expected/smoke.json (MIT)", "rel_tol": 1e-7,
