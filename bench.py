@@ -17,11 +17,19 @@ e2e = the same batched metric through the public API: the batch created from hos
 every step the per-replica observables molecular_dynamics.py's append_sample reads, the
 final positions and velocities read back; wall-clock time of all of it (the batch's
 destruction afterwards is reported in e2e.phases, not timed).
+e2e_long: the same through a 1,000-step session, which amortises the batch's creation.
+dropin_run_loop: one cell driven through MDDriver with the calls the reference's own run
+loop makes per step (integrate() and the 17 reads of append_sample), wall clock.
 time_to_cij (rank 0, --no-cij skips it): wall time to C11/C12/C44 within 2 % of the FP64
 plain protocol's result, the plain protocol (one FP64 cell, NPT then NVT as the reference's
 sample case, 120k steps) against 4 mixed-precision replicas started in the box the trained
-warm-start network proposes (see time_to_cij). --cij-nialco adds the same comparison for
-the 108,000-atom Ni-Al-Co cell and the ternary network (see time_to_cij_nialco).
+warm-start network proposes, and against the same replicas without the network
+(ablation_no_network; see time_to_cij). The same comparison runs for the 108,000-atom
+Ni-Al-Co cell and the ternary network (time_to_cij_nialco; --no-cij-nialco skips it).
+mixed_vs_fp64 (--no-precision-report skips it): the mixed path's error against FP64 on
+the workload cell, per quantity over a same-seed window and for C_ij over paired replicas.
+other_configs: 64 uneven replicas, the 32,000-atom L1_2 cell and configuration C1 (pure
+Cu, single-element Cu01 tables, 500 atoms, FP64).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--replicas R] [--precision fp64|mixed]
@@ -51,6 +59,7 @@ METRIC = "atom-steps/s"
 WORKLOAD = "cuzn6_fcc15_13500_nvt300"
 NSIDE, N_ZN, T_K, DT, SKIN, REBUILD = 15, 810, 300.0, 2e-15, 1.2, 20
 L2_FLUSH_BYTES = 512 << 20
+E2E_LONG = 1000
 
 
 # ----------------------------------------------------------------------------- clocks
@@ -231,6 +240,30 @@ def run_ours(args, rank, world, local_rank):
     if dist is not None:
         dist.all_reduce(t_e2e, op=dist.ReduceOp.MAX)
     e2e_value = atoms_all * e2e_steps / float(t_e2e.item())
+    # the same session over E2E_LONG steps: creation amortised, the per-step API cost shows
+    e2e_long = None
+    if not args.no_e2e:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        bb = make_batch(m, t, cells, dt=DT, r_skin=SKIN, precision=args.precision,
+                        device=local_rank)
+        bb.set_launch(tune["tpa_density"], tune["tpa_force"], tune["blocks_density"],
+                      tune["blocks_force"])
+        t1 = time.perf_counter()
+        for s in range(E2E_LONG):
+            bb.run(1, REBUILD, 1, False)
+            _ = bb.observables_all()
+        t2 = time.perf_counter()
+        for r in range(bb.n_replicas):
+            _ = (bb.atoms(r, m.ATOM_POSITIONS), bb.atoms(r, m.ATOM_VELOCITIES))
+        t3 = time.perf_counter()
+        del bb
+        tl = torch.tensor([t3 - t0], dtype=torch.float64, device="cuda")
+        if dist is not None:
+            dist.all_reduce(tl, op=dist.ReduceOp.MAX)
+        e2e_long = {"value": atoms_all * E2E_LONG / float(tl.item()), "unit": "atom-steps/s",
+                    "steps": E2E_LONG,
+                    "phases": {"create_s": t1 - t0, "steps_s": t2 - t1, "readback_s": t3 - t2}}
     tb = t.phi.size + t.rho.size + t.F.size
     h2d = args.replicas * N * (6 * 8 + 4) + 3 * 8 * tb
     d2h = e2e_steps * args.replicas * (78 * 8 + 8) + args.replicas * 2 * N * 24
@@ -242,8 +275,14 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0 and not args.no_cij:
         cij = time_to_cij(m, t, cpu)
     cij_nialco = None
-    if rank == 0 and args.cij_nialco:
+    if rank == 0 and not args.no_cij and not args.no_cij_nialco:
         cij_nialco = time_to_cij_nialco(m)
+    precision_report = None
+    if rank == 0 and not args.no_precision_report and args.workload == WORKLOAD:
+        precision_report = mixed_vs_fp64(m, t)
+    run_loop = None
+    if rank == 0 and not args.no_e2e and args.workload == WORKLOAD:
+        run_loop = dropin_run_loop(m, t)
     others = None if args.no_configs else other_configs(m, t, local_rank, peak=peak)
     n_rebuilds = (args.steps + REBUILD - 1) // REBUILD
     launches = args.steps * 6 + n_rebuilds * 3
@@ -266,6 +305,7 @@ def run_ours(args, rank, world, local_rank):
         "plain_fp64_single_cell": plain,
         "time_to_cij": cij,
         "time_to_cij_nialco_108000": cij_nialco,
+        "mixed_vs_fp64": precision_report,
         "other_configs": others,
         "roofline": roof,
         "roofline_step": step_roofline(value / world, nbar, peak),
@@ -275,6 +315,8 @@ def run_ours(args, rank, world, local_rank):
             "h2d_bytes_per_step": h2d / e2e_steps, "d2h_bytes_per_step": d2h / e2e_steps,
             "steps": e2e_steps, "api": "md_driver_module.BatchedMDDriver",
             "phases": phases},
+        "e2e_long": e2e_long,
+        "dropin_run_loop": run_loop,
         "gpu_launches": launches,
         "clocks": clocks,
     }
@@ -324,7 +366,85 @@ def other_configs(m, t, device, steps=50, warmup=5, peak=6650.0):
                      "ms_per_step": ms / steps, "launch": tune,
                      "roofline_step": step_roofline(value, batch_nbar(b), peak)}
         del b
+    out[C1_NAME] = c1_config(m, device, peak)
     return out
+
+
+C1_NAME = "cu01_fcc5_500_nvt300_fp64"
+
+
+def c1_config(m, device, peak, steps=1000, warmup=20, replicas=64):
+    """Configuration C1: pure Cu, the single-element Mishin Cu01 tables (10,000 nodes per
+    function), the pure-Cu example's 5x5x5 FCC cell (500 atoms) at the file's lattice
+    constant, NVT 300 K, dt 1 fs, FP64, observables every step, list (r_skin 1.2) every 20
+    steps. One cell through MDDriver (the configuration as stated), and the same cell in
+    64 replicas through BatchedMDDriver; CUDA-event timed, autotuned. The reference core
+    runs the same cell on one host core for comparison (200 steps, list included)."""
+    from mdelast_b200.potentials import find_potential, read_setfl
+    from mdelast_b200.systems import make_batch, make_driver, pure_cell
+    path = find_potential("Cu01.eam.alloy.txt")
+    if path is None:
+        return {"unavailable": "Cu01.eam.alloy.txt not staged"}
+    t = read_setfl(path)
+    cell = pure_cell(t, 5, T=300.0, ensemble=1, velocity_seed=0)
+    d = make_driver(m, t, cell, dt=1e-15, r_skin=SKIN, precision="fp64", device=device)
+    tune = d.autotune(2)
+    d.run(warmup, REBUILD, 1, False)
+    ms = d.run(steps, REBUILD, 1, True)
+    point, _ = d.neighbor_list()
+    nbar = float(point[-1]) / cell.n_atoms
+    value = cell.n_atoms * steps / (ms * 1e-3)
+    out = {"value": value, "unit": "atom-steps/s", "atoms": cell.n_atoms, "replicas": 1,
+           "steps": steps, "ms_per_step": ms / steps, "precision": "fp64", "dt_fs": 1,
+           "potential": "Cu01.eam.alloy.txt", "launch": tune,
+           "roofline_step": step_roofline(value, nbar, peak)}
+    del d
+    cells = [pure_cell(t, 5, T=300.0, ensemble=1, velocity_seed=k) for k in range(replicas)]
+    b = make_batch(m, t, cells, dt=1e-15, r_skin=SKIN, precision="fp64", device=device)
+    tune_b = b.autotune(2)
+    b.run(warmup, REBUILD, 1, False)
+    ms_b = b.run(200, REBUILD, 1, True)
+    vb = b.n_atoms * 200 / (ms_b * 1e-3)
+    out["batched"] = {"value": vb, "unit": "atom-steps/s", "replicas": replicas,
+                      "atoms": b.n_atoms, "steps": 200, "ms_per_step": ms_b / 200,
+                      "precision": "fp64", "launch": tune_b,
+                      "roofline_step": step_roofline(vb, nbar, peak)}
+    del b
+    from oracle import ref
+    if ref.available("ref"):
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(1) as pool:
+            per_step = pool.map(_ref_c1_worker, [200])[0]
+        out["reference_cpu_1core"] = {
+            "value": cell.n_atoms / per_step, "unit": "atom-steps/s", "cores": 1,
+            "kind": "reference", "ms_per_step": per_step * 1e3,
+            "sample": "200 steps of the same cell, list rebuilt every 20 steps (included)"}
+    return out
+
+
+def _ref_c1_worker(n_steps):
+    """The reference core on the C1 cell: n_steps with the 20-step list cadence."""
+    sys.path.insert(0, ROOT)
+    os.dup2(os.open(os.devnull, os.O_WRONLY), 1)
+    import numpy as np
+
+    from mdelast_b200.potentials import find_potential, read_setfl
+    from mdelast_b200.systems import pure_cell, rg_bins
+    from oracle.ref import RefDriver
+    t = read_setfl(find_potential("Cu01.eam.alloy.txt"))
+    c = pure_cell(t, 5, T=300.0, ensemble=1, velocity_seed=0)
+    d = RefDriver(t, c.positions, c.velocities, c.types, ensemble=1,
+                  thermo=(c.T, c.thermo_q, c.thermo_p_eta, c.Nf),
+                  baro=(c.pressure, c.baro_w, c.baro_p_eps),
+                  baro_thermo=(c.T, c.baro_q, c.baro_p_eta, 1.0),
+                  box=np.diag(c.box), rg=rg_bins(c, 3.615), Nf=c.Nf, dt=1e-15,
+                  neighbors=True, r_skin=SKIN)
+    t0 = time.perf_counter()
+    for k in range(n_steps):
+        if k % REBUILD == 0:
+            d.calculate_neighbors()
+        d.integrate()
+    return (time.perf_counter() - t0) / n_steps
 
 
 WORKLOADS = {WORKLOAD: "NVT 300 K", "l12_cuzn3_20x20x20_32000_nvt5": "NVT 5 K"}
@@ -390,6 +510,7 @@ def time_to_cij(m, t, cpu):
     t_warm = time_to_within(warm, target, CIJ_TOL)
     t_warm = None if t_warm is None else setup + t_warm
     t_plain_self = time_to_within(plain, target, CIJ_TOL)
+    ablation = ablation_no_network(m, t, target)
     out = {
         "metric": f"wall time to C11/C12/C44 within {CIJ_TOL:.0%} of the FP64 plain result",
         "unit": "s", "cell": WORKLOAD, "tolerance": CIJ_TOL,
@@ -407,6 +528,9 @@ def time_to_cij(m, t, cpu):
         "speedup_vs_plain_protocol": (plain.wall_s / t_warm) if t_warm else None,
         "speedup_vs_plain_time_to_within": (t_plain_self / t_warm)
         if (t_warm and t_plain_self) else None,
+        "ablation_no_network": ablation,
+        "network_gain_vs_ablation": (ablation["time_to_within_s"] / t_warm)
+        if (t_warm and ablation.get("time_to_within_s")) else None,
     }
     if cpu and cpu.get("value"):
         # the reference core's measured per-step time on this host, times the plain protocol
@@ -418,6 +542,30 @@ def time_to_cij(m, t, cpu):
         if t_warm:
             out["speedup_vs_reference_cpu_estimated"] = est / t_warm
     return out
+
+
+ABLATION_STAGES = dict(npt_therm=1000, npt_prod=1000, nvt_therm=500, nvt_prod=3000,
+                       sample_stride=5, rebuild_every=REBUILD, checkpoint_every=250)
+
+
+def ablation_no_network(m, t, target):
+    """The warm start without its network: the same 4 mixed-precision replicas (same
+    seeds, same NVT stages and checkpoints) started at the linear (Vegard) lattice constant
+    with a short NPT stage (1,000 + 1,000 steps) to find the box. Its time to within 2 % of
+    the plain result, set against the warm start's, is what the network contributes."""
+    from mdelast_b200.protocol import Stages, run_protocol, time_to_within
+    from mdelast_b200.systems import cuzn_cell, vegard_a
+    x = N_ZN / NSIDE**3 / 4
+    a = vegard_a(x, T_K)
+    cells = [cuzn_cell(t, NSIDE, n_zn=N_ZN, T=T_K, a_ang=a, ensemble=2, placement_seed=42,
+                       velocity_seed=200 + k) for k in range(WARM_REPLICAS)]
+    res = run_protocol(m, t, cells, precision="mixed", stages=Stages(**ABLATION_STAGES),
+                       nvt_seeds=[300 + k for k in range(WARM_REPLICAS)])
+    tw = time_to_within(res, target, CIJ_TOL)
+    return {"time_to_within_s": tw, "wall_s": res.wall_s, "wall_npt_s": res.wall_npt_s,
+            "C_GPa": res.C, "rel_err_vs_plain": {k: res.C[k] / target[k] - 1 for k in target},
+            "a_start": a, "npt_mean_V_V0": res.V_V0, "stages": ABLATION_STAGES,
+            "replicas": WARM_REPLICAS}
 
 
 NIALCO_NSIDE = 30  # 108,000 atoms
@@ -479,6 +627,131 @@ def time_to_cij_nialco(m):
         "speedup_vs_plain_time_to_within": (t_plain_self / t_warm)
         if (t_warm and t_plain_self) else None,
     }
+
+
+A_EQ_300K = 3.66683  # [A] FP64 NPT production mean of the 13,500-atom cell at 300 K
+
+
+def mixed_vs_fp64(m, t, window=200, replicas=4, therm=2000, prod=20000):
+    """Error of the mixed-precision path against the FP64 path on the timed workload cell.
+
+    same_seed_window: one cell (velocity seed 0) run in both precisions from the same
+    state for `window` steps, observables sampled every step; per quantity the largest
+    deviation of the mixed run from the FP64 run over the first 10, 50 and `window` steps
+    (relative for energies and temperatures, in GPa for pressure and stresses, which pass
+    through zero). Trajectories that differ by rounding diverge exponentially, so the
+    short windows measure the arithmetic and the long one the start of the divergence.
+
+    cij: `replicas` cells at the FP64 NPT mean lattice constant of this cell at 300 K
+    (A_EQ_300K), velocity seeds 100.., run in both precisions (NVT 300 K,
+    `therm` steps, then C11/C12/C44 by the fluctuation formula over `prod` steps sampled
+    every step). Reported: each precision's mean over replicas with its standard error, and
+    the paired difference mixed - FP64 with its standard error (the trajectories decorrelate
+    long before the end of production, so the pairs are independent samples)."""
+    import numpy as np
+
+    from mdelast_b200.systems import cuzn_cell, make_batch, make_driver
+    from mdelast_b200.units import Units as U
+    cell = cuzn_cell(t, NSIDE, n_zn=N_ZN, T=T_K, ensemble=1, placement_seed=42, velocity_seed=0)
+    recs = {}
+    for prec in ("fp64", "mixed"):
+        d = make_driver(m, t, cell, dt=DT, r_skin=SKIN, precision=prec)
+        d.run(window, REBUILD, 1, False)
+        recs[prec] = d.drain_samples()
+        del d
+    a, b = recs["mixed"], recs["fp64"]
+    eV = U.ev
+    quantities = {
+        "epot_atom": ("rel", a["epot_atom"], b["epot_atom"]),
+        "etot_cons": ("rel", a["etot_cons"], b["etot_cons"]),
+        "temperature_kin": ("rel", a["temperature_kin"], b["temperature_kin"]),
+        "temperature_conf": ("rel", 1.0 / a["temperature_conf_inverse"],
+                             1.0 / b["temperature_conf_inverse"]),
+        "pressure_GPa": ("abs", a["pressure"] / U.GPa, b["pressure"] / U.GPa),
+        "born_stress_GPa": ("abs", a["born_stress_tensor"] / U.GPa,
+                            b["born_stress_tensor"] / U.GPa),
+        "born_elasticity_GPa": ("abs", a["born_elasticity_tensor"] / U.GPa,
+                                b["born_elasticity_tensor"] / U.GPa),
+    }
+    win = {}
+    for name, (kind, x, y) in quantities.items():
+        x, y = np.asarray(x), np.asarray(y)
+        dev = np.abs(x - y)
+        if kind == "rel":
+            dev = dev / np.abs(y)
+        dev = dev.reshape(len(dev), -1).max(axis=1)
+        win[name] = {f"max_first_{n}": float(dev[:n].max()) for n in (10, 50, window)}
+        win[name]["kind"] = "relative" if kind == "rel" else "absolute"
+    win["epot_atom_eV_first_step"] = [float(a["epot_atom"][0] / eV), float(b["epot_atom"][0] / eV)]
+
+    cells = [cuzn_cell(t, NSIDE, n_zn=N_ZN, T=T_K, a_ang=A_EQ_300K, ensemble=1,
+                       placement_seed=42, velocity_seed=100 + k) for k in range(replicas)]
+    C = {}
+    wall = {}
+    for prec in ("fp64", "mixed"):
+        t0 = time.perf_counter()
+        bt = make_batch(m, t, cells, dt=DT, r_skin=SKIN, precision=prec)
+        bt.autotune(2)
+        bt.set_sample_ring(0)
+        bt.run(therm, REBUILD, 1, False)
+        bt.fluctuation_start()
+        bt.run(prod, REBUILD, 1, False)
+        C[prec] = np.array([[bt.elastic_constants(r)[k] / U.GPa for k in ("C11", "C12", "C44")]
+                            for r in range(replicas)])
+        wall[prec] = time.perf_counter() - t0
+        del bt
+    diff = C["mixed"] - C["fp64"]
+    se = lambda x: (x.std(axis=0, ddof=1) / np.sqrt(len(x))).tolist()  # noqa: E731
+    names = ("C11", "C12", "C44")
+    cij = {"replicas": replicas, "thermalisation_steps": therm, "production_steps": prod,
+           "sample_every": 1, "unit": "GPa", "wall_s": wall}
+    for prec in ("fp64", "mixed"):
+        cij[prec] = {k: {"mean": float(C[prec][:, i].mean()), "se": float(se(C[prec])[i])}
+                     for i, k in enumerate(names)}
+    cij["mixed_minus_fp64"] = {k: {"mean": float(diff[:, i].mean()), "se": float(se(diff)[i]),
+                                   "rel": float(diff[:, i].mean() / C["fp64"][:, i].mean())}
+                               for i, k in enumerate(names)}
+    return {"cell": WORKLOAD, "same_seed_window": win, "window_steps": window, "cij": cij}
+
+
+def run_loop_calls(d, steps, rebuild=REBUILD):
+    """The calls MolecularDynamics.run() makes on its driver per step, in its order
+    (molecular_dynamics.py:1240-1285, observables sampled every step): the cycle checks,
+    the list rebuild every `rebuild` steps, sample_observables, integrate(), then the reads
+    of append_sample (molecular_dynamics.py:1218-1238)."""
+    import numpy as np
+    for _ in range(steps):
+        c = d.cycle
+        if c % rebuild == 0:
+            d.calculate_neighbors()
+        d.sample_observables = True
+        d.integrate()
+        _ = (d.time, d.temperature_kin, d.temperature_conf_inverse, d.total_laplacian,
+             d.total_force2, d.pressure, np.copy(d.stress_tensor), d.etot_atom, d.epot_atom,
+             d.epot_eam_atom, d.ekin_atom, d.etot_cons, d.etot_cons_err,
+             np.copy(d.born_stress_tensor), np.copy(d.born_elasticity_tensor),
+             d.box.volume() / d.box_initial.volume(), d.cycle)
+
+
+def dropin_run_loop(m, t, steps=200, warmup=20):
+    """Atom-steps/s of the workload cell driven the way the reference's run loop drives
+    its driver (run_loop_calls): one MDDriver, one integrate() per step and 17 attribute
+    reads after it, wall-clock time; FP64 and mixed precision."""
+    from mdelast_b200.systems import cuzn_cell, make_driver
+    cell = cuzn_cell(t, NSIDE, n_zn=N_ZN, T=T_K, ensemble=1, placement_seed=42, velocity_seed=0)
+    out = {"api": "md_driver_module.MDDriver, the calls of molecular_dynamics.py:1240-1285",
+           "atoms": cell.n_atoms, "steps": steps, "unit": "atom-steps/s"}
+    for prec in ("fp64", "mixed"):
+        d = make_driver(m, t, cell, dt=DT, r_skin=SKIN, precision=prec)
+        d.autotune(2)
+        run_loop_calls(d, warmup)
+        d.synchronize()
+        t0 = time.perf_counter()
+        run_loop_calls(d, steps)
+        wall = time.perf_counter() - t0
+        out[prec] = {"value": cell.n_atoms * steps / wall, "ms_per_step": 1e3 * wall / steps}
+        del d
+    return out
 
 
 def half_list_nbar(m, t, cell):
@@ -600,9 +873,11 @@ def main():
                     help="skip the other workloads (64 uneven replicas, L1_2 32k cell)")
     ap.add_argument("--no-cij", action="store_true",
                     help="skip the time-to-C_ij comparison (plain FP64 protocol vs warm start)")
-    ap.add_argument("--cij-nialco", action="store_true",
-                    help="also time C_ij of the 108,000-atom Ni-Al-Co cell: plain FP64 "
-                         "protocol vs the ternary warm start (adds about 3 minutes)")
+    ap.add_argument("--no-cij-nialco", action="store_true",
+                    help="skip the C_ij timing of the 108,000-atom Ni-Al-Co cell (plain FP64 "
+                         "protocol vs the ternary warm start; about 3 minutes)")
+    ap.add_argument("--no-precision-report", action="store_true",
+                    help="skip the mixed-vs-FP64 error report (about 30 s)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

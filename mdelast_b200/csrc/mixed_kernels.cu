@@ -1,6 +1,7 @@
 // Mixed-precision pair passes: pair geometry and table evaluation in FP32, in angstrom and
-// eV, with every sum over pairs (per-atom forces and energies, the virial, Born stress,
-// Born tensor and Laplacian) accumulated in FP64 and converted to cgs at the end.
+// eV, with every sum over pairs (per-atom densities, forces and energies, the virial, Born
+// stress, Born tensor and Laplacian) accumulated in FP64 and converted to cgs at the end;
+// the per-atom helpers g_i and h_i of the density pass are summed in FP32 along the row.
 //
 // Pair forces stay exactly antisymmetric: dp_ij = -dp_ji bit for bit (IEEE subtraction and
 // round-to-nearest-even are odd functions), every other pair quantity depends on r only,
@@ -159,7 +160,7 @@ __global__ void __launch_bounds__(kBlock) k_density_mx(AtomsView A, TablesView T
         int const a = a0 + static_cast<int>(threadIdx.x) / TPA;
         int const i = R->atom_begin + a;
         bool const valid = a < R->n_atoms && T.has_eam;
-        float rho = 0.f;
+        double rho = 0.;
         float g[6] = {0, 0, 0, 0, 0, 0}, hv[3] = {0, 0, 0};
         int ti = 0;
         if (valid) {
@@ -187,7 +188,7 @@ __global__ void __launch_bounds__(kBlock) k_density_mx(AtomsView A, TablesView T
                 tabf_eval<IP, true, OBS, false>(
                     T.rrf + (static_cast<size_t>(tj) * T.nri + k) * TabFmt<IP>::kFf, t,
                     T.finv_hr, T.finv_hr2, v, d1, d2);
-                rho += v;
+                rho += static_cast<double>(v);
                 if (OBS) {
                     float const ar = d1 * idr;
                     float const ap[3] = {ar * dx, ar * dy, ar * dz};
@@ -216,7 +217,7 @@ __global__ void __launch_bounds__(kBlock) k_density_mx(AtomsView A, TablesView T
         bool const own = valid && sub == 0;
         if (own) {
             // the embedding function in FP64 and cgs (eam.hpp:48-70)
-            double const rc = static_cast<double>(rho) / a3;
+            double const rc = rho / a3;
             if (rc > T.rhomax[ti])
                 status_or(A.rep + r, MDELAST_FATAL_RHO_MAX);
             double t;

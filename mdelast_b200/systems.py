@@ -7,6 +7,8 @@ reference's cgs units. The builders restate the reference's scripts:
   224-227``): the 500-atom sample case, the 13,500-atom 15x15x15 cell, or any size and
   composition;
 * :func:`l12_cell` - ordered L1_2 CuZn3 (``benchmarks/l12_cuzn3_5K/run.py:78-92``);
+* :func:`pure_cell` - one element on an FCC lattice, the pure-Cu example
+  (``examples/cu_300k/run.py:58-78``) with the single-element Cu01 tables;
 * :func:`uneven_replicas` - independent cells of 4 n^3 atoms with n uniform in [4, 20], Zn
   fraction uniform in [0, 0.30], temperature uniform in [5, 900] K, separate seeds, drawn
   from one master ``RandomState``.
@@ -103,6 +105,17 @@ def l12_cell(tables: SetflTables, n: int, T: float = 5.0, ensemble: int = 1,
     pos, types, L = l12_lattice(a_ang * U.angstrom, n, names.index("Zn"), names.index("Cu"))
     return _state(tables, pos, types, [L] * 3, T, ensemble, velocity_seed,
                   {"kind": "l12_cuzn3", "n": n, "a_ang": a_ang})
+
+
+def pure_cell(tables: SetflTables, nside: int = 5, T: float = 300.0, ensemble: int = 1,
+              velocity_seed: int = 0, a_ang: float | None = None) -> Cell:
+    """FCC cell of the potential's first element at the file's lattice constant (the
+    value ``get_EAM_file`` hands to ``Material``), or ``a_ang``."""
+    a = tables.meta.get("a_lattice", A0_CU * U.angstrom) if a_ang is None else a_ang * U.angstrom
+    pos, L = fcc_lattice(nside, a)
+    types = np.zeros(len(pos), dtype=np.uint32)
+    return _state(tables, pos, types, [L] * 3, T, ensemble, velocity_seed,
+                  {"kind": "pure_fcc", "nside": nside, "a_ang": a / U.angstrom})
 
 
 def vegard_a(x_zn: float, T: float) -> float:

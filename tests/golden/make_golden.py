@@ -7,8 +7,8 @@ checkout called ``reference`` beside this repository):
 
 Writes
 * ``smoke_static.json``: benchmark S Part A6 expected values per table interpolation
-  (``benchmarks/expected/smoke.json:34-88``, rel tol 1e-7), and the Part C bounds
-  (``smoke.json:90-113``);
+  (``benchmarks/expected/smoke.json:34-88``, rel tol 1e-7), the Part A and C bounds
+  (``smoke.json:6-33, 90-113``) and the Part B dynamics bounds (``smoke.json:114-170``);
 * ``nialco_lammps.npz``: the fixed 500-atom Ni-Al-Co cell and the LAMMPS values it is checked
   against (``benchmarks/smoke/reference/``), converted as ``run_smoke.py:281-328`` does:
   positions [A] wrapped into the box, 0-based types, forces [eV/A], energy [eV/atom],
@@ -53,6 +53,8 @@ def main():
                 out[interp][k[len("static."):]] = v["expected_by_interpolation"][interp]
         elif k.startswith("ternary.") or k.startswith("static."):
             out["bounds"][k] = v.get("max")
+        elif k.startswith("dynamics."):
+            out.setdefault("dynamics_bounds", {})[k] = {b: v[b] for b in ("min", "max") if b in v}
     json.dump(out, open(os.path.join(HERE, "smoke_static.json"), "w"), indent=1, sort_keys=True)
 
     refdir = os.path.join(a.ref, "benchmarks", "smoke", "reference")

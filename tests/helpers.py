@@ -18,11 +18,12 @@ _TABLES = {}
 
 
 def tables(name="ZnCu.eam.alloy"):
-    """Node arrays of a potential from the copies the oracle recipe makes; skip if absent."""
+    """Node arrays of a potential staged by the build (or under $MDELAST_POTENTIALS);
+    skip if absent."""
     if name not in _TABLES:
         path = find_potential(name)
         if path is None:
-            pytest.skip(f"potential {name} not available (make -C oracle potentials)")
+            pytest.skip(f"potential {name} not staged (python -m mdelast_b200.build)")
         _TABLES[name] = read_setfl(path)
     return _TABLES[name]
 
@@ -192,3 +193,32 @@ def gpu_atoms(d, field):
             "velocities": m.ATOM_VELOCITIES, "forces": m.ATOM_FORCES, "rho_eam": m.ATOM_RHO,
             "energies_pot": m.ATOM_EPOT, "energies_kin": m.ATOM_EKIN}[field]
     return np.asarray(d.atoms_array(code))
+
+
+CU01 = "Cu01.eam.alloy.txt"
+
+
+def cu01_case(nside=5, ensemble=1, T=300.0, dt=1e-15, seed=0, neighbors=True, r_skin=1.2,
+              sigma_ang=0.0, displace_seed=2026) -> Case:
+    """Pure Cu with the single-element Mishin Cu01 tables (10,000 nodes): the pure-Cu
+    example's FCC cell at the file's lattice constant (``examples/cu_300k/run.py:58-78``,
+    ``get_EAM_file``), 300 K, dt 1 fs. ``sigma_ang`` > 0 displaces every atom by a seeded
+    Gaussian (a static cell with non-zero forces)."""
+    t = tables(CU01)
+    a = t.meta["a_lattice"]
+    pos, L = fcc_lattice(nside, a)
+    if sigma_ang > 0:
+        rs = np.random.RandomState(displace_seed)
+        pos = pos + rs.normal(scale=sigma_ang * U.angstrom, size=pos.shape)
+        pos = np.mod(pos + L / 2, L) - L / 2
+    typ = np.zeros(len(pos), dtype=int)
+    mass = np.array(t.masses)[typ]
+    st = initial_state(mass, T, T, 5e-14, 5e-13, random_seed=seed)
+    drg = a / 500
+    ng = int(L / 2.0 / drg)
+    return Case(t, pos, st.velocities, typ, np.diag([L] * 3), ensemble=ensemble,
+                thermo=(T, st.thermo_q, st.thermo_p_eta, st.Nf),
+                baro=(1e-10 * U.GPa, st.baro_w, st.baro_p_eps),
+                baro_thermo=(T, st.baro_q, st.baro_p_eta, 1.0),
+                rg=[(k + 0.5) * drg for k in range(ng)], Nf=st.Nf, dt=dt,
+                neighbors=neighbors, r_skin=r_skin)

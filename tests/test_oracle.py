@@ -152,3 +152,26 @@ def test_oracle_bitwise_bspline(maker):
     b.integrate(10)
     assert np.array_equal(a.scalars(), b.scalars())
     assert np.array_equal(a.atoms("forces"), b.atoms("forces"))
+
+
+@needs_ref
+@needs_oracle
+def test_oracle_bitwise_cu01():
+    """Pure Cu with the single-element 10,000-node Cu01 tables (the pure-Cu example):
+    a displaced static cell and 20 NVT steps with a list rebuild, bit-identical."""
+    from helpers import cu01_case
+    c = cu01_case(sigma_ang=0.08)
+    a, b = oracle(c, "ref"), oracle(c, "oracle")
+    assert np.array_equal(a.scalars(), b.scalars())
+    assert np.array_equal(a.atoms("forces"), b.atoms("forces"))
+    c = cu01_case()
+    a, b = oracle(c, "ref"), oracle(c, "oracle")
+    for step in range(20):
+        if step % 10 == 0:
+            a.calculate_neighbors()
+            b.calculate_neighbors()
+        a.integrate()
+        b.integrate()
+    assert np.array_equal(a.scalars(), b.scalars())
+    for f in ("positions", "velocities", "forces"):
+        assert np.array_equal(a.atoms(f), b.atoms(f))
