@@ -66,9 +66,10 @@ const char *mdelast_last_error(void);
 int mdelast_abi_version(void);
 /* 1 when a CUDA device is usable, 0 otherwise (no error). */
 int mdelast_device_available(void);
-/* Drivers take their device buffers from the device's default stream-ordered memory pool,
- * which keeps freed memory for the next driver; this hands the unused part of it back to
- * the device. No reference counterpart (the reference holds host memory only). */
+/* Drivers take their device buffers from a stream-ordered memory pool of the library's
+ * own (one per device; the device's default pool is not touched), which keeps freed memory
+ * for the next driver; this hands the unused part of it back to the device. No reference
+ * counterpart (the reference holds host memory only). */
 int mdelast_release_cached_memory(int32_t device);
 
 /* ---------------------------------------------------------------------------------
@@ -390,8 +391,9 @@ int mdelast_mlp_train(mdelast_mlp *m, const float *x, const float *y, int32_t n,
  * Same counting and normalisation as mdelast_driver_pair_correlation (md_driver.cpp:
  * 732-862) and bit-identical results on the same coordinates, but on arrays the caller
  * holds on the current device: coordinates (n_atoms x 3 scaled coordinates, as the
- * MDELAST_ATOM_COORDINATES readout), types (n_atoms values in [0, n_types); atoms of other
- * types are not counted), rg (n_rg evenly spaced bin centres, rg[0] > 0), and the outputs
+ * MDELAST_ATOM_COORDINATES readout), types (n_atoms values; an atom whose type is not in
+ * [0, n_types) takes no part: it is in no pair count and not in the N of the
+ * normalisations), rg (n_rg evenly spaced bin centres, rg[0] > 0), and the outputs
  * gr (n_rg, written for modes 0 and 1) and gr_partial (n_types(n_types+1)/2 rows of n_rg,
  * written for modes 1 and 2; the other may be NULL). box: 3 edges of the diagonal box, in
  * host memory. The work is queued on `stream` (a cudaStream_t; NULL is the default stream)
@@ -405,7 +407,10 @@ int mdelast_mlp_train(mdelast_mlp *m, const float *x, const float *y, int32_t n,
  *
  * The first call on a device does set-up (it loads the library's kernels on that device
  * and looks up the scratch address with cudaGetSymbolAddress, with that device current);
- * make it before any stream capture begins. There is ONE scratch array per device: calls
+ * make it before any stream capture begins. The address is kept for the life of the
+ * process: after a cudaDeviceReset of that device it is stale, and this entry point must
+ * not be used on that device again in the same process. There is ONE scratch array per
+ * device: calls
  * that overlap on the same device (different streams, or different host threads, without
  * ordering between them) race on it and give wrong counts; order them on one stream or
  * with events. */

@@ -29,26 +29,33 @@ using namespace mdelast;
 
 namespace {
 
-// Device buffers come from the device's default stream-ordered memory pool, whose release
-// threshold is raised once per device so that the process keeps freed memory: a driver
+// Device buffers come from a stream-ordered memory pool of this library's own, one per
+// device, created on first use with a release threshold that keeps freed memory: a driver
 // created after another was destroyed (the NPT and NVT stages of a protocol, a warm start's
-// corrected boxes) reuses its pages instead of mapping new ones.
-// mdelast_release_cached_memory() hands the unused part back to the device.
-int keep_pool(int dev) {
-    static std::mutex mu;
-    static std::vector<char> done;
-    std::lock_guard<std::mutex> lock(mu);
+// corrected boxes) reuses its pages instead of mapping new ones. The device's default pool,
+// which other users in the process (PyTorch's cudaMallocAsync backend, for one) may tune
+// for themselves, is left as it is. mdelast_release_cached_memory() trims this pool.
+std::mutex g_pool_mutex;
+std::vector<cudaMemPool_t> g_pools;
+
+int own_pool(int dev, cudaMemPool_t *out) {
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
     if (dev < 0)
-        return MDELAST_OK;
-    if (done.size() <= static_cast<size_t>(dev))
-        done.resize(static_cast<size_t>(dev) + 1, 0);
-    if (done[static_cast<size_t>(dev)])
-        return MDELAST_OK;
-    cudaMemPool_t pool;
-    CK(cudaDeviceGetDefaultMemPool(&pool, dev));
-    uint64_t keep = UINT64_MAX;
-    CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
-    done[static_cast<size_t>(dev)] = 1;
+        return fail(MDELAST_ERR_ARGUMENT, "device %d", dev);
+    if (g_pools.size() <= static_cast<size_t>(dev))
+        g_pools.resize(static_cast<size_t>(dev) + 1, nullptr);
+    cudaMemPool_t &pool = g_pools[static_cast<size_t>(dev)];
+    if (!pool) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        CK(cudaMemPoolCreate(&pool, &props));
+        uint64_t keep = UINT64_MAX;
+        CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    }
+    *out = pool;
     return MDELAST_OK;
 }
 
@@ -58,9 +65,10 @@ template <typename T> int dalloc(T **p, size_t n) {
     size_t const bytes = sizeof(T) * (n > 0 ? n : 1);
     int dev = 0;
     CK(cudaGetDevice(&dev));
-    if (int rc = keep_pool(dev))
+    cudaMemPool_t pool = nullptr;
+    if (int rc = own_pool(dev, &pool))
         return rc;
-    CK(cudaMallocAsync(reinterpret_cast<void **>(p), bytes, cudaStreamLegacy));
+    CK(cudaMallocFromPoolAsync(reinterpret_cast<void **>(p), bytes, pool, cudaStreamLegacy));
     CK(cudaMemsetAsync(*p, 0, bytes, cudaStreamLegacy));
     CK(cudaStreamSynchronize(cudaStreamLegacy));
     return MDELAST_OK;
@@ -726,9 +734,14 @@ int mdelast_release_cached_memory(int32_t device) {
         return fail(MDELAST_ERR_ARGUMENT, "device %d out of range", device);
     CK(cudaSetDevice(device));
     CK(cudaDeviceSynchronize());
-    cudaMemPool_t pool;
-    CK(cudaDeviceGetDefaultMemPool(&pool, device));
-    CK(cudaMemPoolTrimTo(pool, 0));
+    cudaMemPool_t pool = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_pool_mutex);
+        if (static_cast<size_t>(device) < g_pools.size())
+            pool = g_pools[static_cast<size_t>(device)];
+    }
+    if (pool)
+        CK(cudaMemPoolTrimTo(pool, 0));
     return MDELAST_OK;
 }
 
@@ -1485,6 +1498,10 @@ static int pair_correlation_r(mdelast_driver *d, int r, int32_t mode) {
     clear_error();
     if (!d || r < 0 || r >= d->n_rep || mode < 0 || mode > 2)
         return fail(MDELAST_ERR_ARGUMENT, "bad argument");
+    if (!gr_atoms_fit(d->rep_count[r]))
+        return fail(MDELAST_ERR_CAPACITY,
+                    "g(r) of %d atoms needs more than 2^31 - 1 blocks of 128-atom tile pairs",
+                    d->rep_count[r]);
     CK(cudaSetDevice(d->device));
     if (int rc = d->wait_step())
         return rc;

@@ -20,7 +20,7 @@ namespace mdelast {
 
 namespace {
 
-constexpr int kGrTile = 128;
+constexpr int kGrTile = static_cast<int>(kGrTileAtoms);
 constexpr size_t kGrSharedMax = 96 * 1024;
 
 // block index q -> tile pair (I, J), I <= J, rows of the upper triangle of T x T tiles
@@ -152,8 +152,7 @@ cudaError_t gr_enqueue(GrArgs const &g, cudaStream_t s) {
     if (e != cudaSuccess)
         return e;
     if (g.n >= 2) {
-        long const T = (g.n + kGrTile - 1) / kGrTile;
-        long const blocks = T * (T + 1) / 2;
+        long const blocks = gr_count_blocks(g.n);
         size_t const tile_bytes = sizeof(double4) * kGrTile;
         size_t const hist_bytes = sizeof(unsigned) * nbins;
         int const shared_hist = tile_bytes + hist_bytes <= kGrSharedMax ? 1 : 0;

@@ -24,6 +24,14 @@ struct GrArgs {
 __host__ __device__ inline size_t gr_count_slots(int n_rg, int ntypes) {
     return static_cast<size_t>(1 + ntypes * (ntypes + 1) / 2) * static_cast<size_t>(n_rg);
 }
+// Thread blocks of the pair count for n atoms: one per pair of 128-atom tiles (I <= J).
+// A launch takes at most 2^31 - 1 blocks, so callers reject n beyond gr_max_atoms().
+constexpr long kGrTileAtoms = 128;
+__host__ inline long gr_count_blocks(long n) {
+    long const T = (n + kGrTileAtoms - 1) / kGrTileAtoms;
+    return T * (T + 1) / 2;
+}
+__host__ inline bool gr_atoms_fit(long n) { return gr_count_blocks(n) <= 2147483647L; }
 // Clears the scratch, counts the pairs, normalises. Asynchronous on stream s; gr is left
 // untouched for mode 2 and gr_partial for mode 0, as in the reference.
 cudaError_t gr_enqueue(GrArgs const &g, cudaStream_t s);

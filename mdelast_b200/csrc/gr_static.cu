@@ -151,7 +151,12 @@ __global__ void k_gr_static_norm(StaticArgs g) {
     double const drg = __dadd_rn(g.rg[1], -g.rg[0]);
     double const r = g.rg[k];
     if (g.mode == 0 || g.mode == 1) {
-        double const nd = static_cast<double>(g.n);
+        // N of the total's normalisation: the atoms counted (those with a type in range),
+        // which is n_atoms whenever every type is valid
+        unsigned long long nv = 0;
+        for (int a = 0; a < g.ntypes; ++a)
+            nv += g.n_per_type[a];
+        double const nd = static_cast<double>(nv);
         double const den =
             __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(2. * pi, nd), nd), r), r), drg);
         g.gr[k] = __dmul_rn(static_cast<double>(g.counts[k]), __ddiv_rn(V, den));
@@ -230,6 +235,11 @@ extern "C" int mdelast_pair_correlation_static(const double *coordinates, const 
                     "%d bins x %d histograms need %zu counters; the static g(r) scratch holds "
                     "%zu (MDELAST_GR_STATIC_MAX_SLOTS)",
                     n_rg, 1 + n_types * (n_types + 1) / 2, nslots, kStaticSlots);
+    long const T = (static_cast<long>(n_atoms) + kTileS - 1) / kTileS;
+    if (T * (T + 1) / 2 > 2147483647L)
+        return fail(MDELAST_ERR_CAPACITY,
+                    "g(r) of %d atoms needs more than 2^31 - 1 blocks of %d-atom tile pairs",
+                    n_atoms, kTileS);
     cudaStream_t const s = static_cast<cudaStream_t>(stream);
     unsigned long long *scratch = nullptr;
     if (int rc = scratch_for_current_device(&scratch))
@@ -253,7 +263,6 @@ extern "C" int mdelast_pair_correlation_static(const double *coordinates, const 
     int const ns = static_cast<int>(nslots);
     k_gr_static_clear<<<(ns + 255) / 256, 256, 0, s>>>(g, ns);
     if (n_atoms >= 2) {
-        long const T = (n_atoms + kTileS - 1) / kTileS;
         size_t const tile_bytes = sizeof(double4) * kTileS;
         size_t const hist_bytes = sizeof(unsigned) * nslots;
         int const shared_hist = tile_bytes + hist_bytes <= kSharedMaxS ? 1 : 0;

@@ -1,7 +1,9 @@
 """mdelast_pair_correlation_static (g(r) with its scratch in a static device array, no
 allocation) against the driver's g(r) entry point on the same coordinates: bit-identical,
-as every g(r) comparison here, on two calls in a row and in all three modes; requests
-beyond the static scratch are rejected before any device work."""
+as every g(r) comparison here, on two calls in a row and in all three modes; on a side
+stream, and with atoms whose type is out of range, against a NumPy restatement of the
+reference's counting (md_driver.cpp:732-811) over the atoms in range; requests beyond the
+static scratch or the launch grid are rejected before any device work."""
 
 import ctypes as C
 import os
@@ -46,6 +48,98 @@ def test_static_scratch_limits_rejected():
     rc = f(crd.ctypes.data, typ.ctypes.data, 4, 9, box, rg.ctypes.data, 10, 0,
            out.ctypes.data, None, None)
     assert rc == ERR_CAPACITY
+
+
+def test_grid_limit_rejected():
+    """More than 2^31 - 1 tile-pair blocks: rejected with the sizes in the message."""
+    lib = _lib()
+    f = lib.mdelast_pair_correlation_static
+    crd = np.zeros((4, 3))
+    typ = np.zeros(4, dtype=np.uint32)
+    box = (C.c_double * 3)(1.0, 1.0, 1.0)
+    rg = np.arange(10, dtype=float) + 0.5
+    out = np.zeros(10)
+    n = 65536 * 128 + 1  # 65,537 tiles: 2,147,549,953 tile pairs
+    rc = f(crd.ctypes.data, typ.ctypes.data, n, 1, box, rg.ctypes.data, 10, 0,
+           out.ctypes.data, None, None)
+    assert rc == ERR_CAPACITY
+    assert "2^31" in lib.mdelast_last_error().decode()
+
+
+def numpy_gr(crd, types, n_types, h, rg, mode):
+    """md_driver.cpp:732-811 in NumPy over the atoms whose type is in [0, n_types): pairs
+    i < j, the reference's min image, bin floor(r / drg) for r < rmaxg, and its
+    normalisations in its operation order; N = the atoms in range."""
+    keep = types < n_types
+    c, t = crd[keep], types[keep].astype(np.int64)
+    n = len(c)
+    drg = rg[1] - rg[0]
+    rmaxg = rg[-1] + 0.5 * drg
+    i, j = np.triu_indices(n, 1)
+    d = c[i] - c[j]
+    d = d - np.where(d < 0, np.trunc(d - 0.5), np.trunc(d + 0.5))
+    p = d * h
+    r = np.sqrt((p[:, 0] * p[:, 0] + p[:, 1] * p[:, 1]) + p[:, 2] * p[:, 2])
+    ok = r < rmaxg
+    b = np.floor(r[ok] / drg).astype(np.int64)
+    V = h[0] * (h[1] * h[2])
+    gr = np.bincount(b, minlength=len(rg)).astype(float)
+    gr = gr * (V / (2.0 * np.pi * n * n * rg * rg * drg))
+    ti, tj = t[i][ok], t[j][ok]
+    hi, lo = np.maximum(ti, tj), np.minimum(ti, tj)
+    slot = hi * (hi + 1) // 2 + lo
+    npair = n_types * (n_types + 1) // 2
+    gp = np.zeros((npair, len(rg)))
+    cnt = np.bincount(slot * len(rg) + b, minlength=npair * len(rg)).reshape(npair, -1)
+    Nt = np.bincount(t, minlength=n_types).astype(float)
+    s = 0
+    for bb in range(n_types):
+        for a in range(bb + 1):
+            Na, Nb = Nt[a], Nt[bb]
+            pc = (Na * (Na - 1.0) / 2.0 if Na > 1 else 0.0) if a == bb else Na * Nb
+            if pc > 0.0:
+                pref = V / (4.0 * np.pi * pc * drg)
+                gp[s] = cnt[s] * (pref / (rg * rg))
+            s += 1
+    return gr, gp
+
+
+@pytest.mark.gpu
+def test_side_stream_and_types_out_of_range():
+    """A torch side stream passed as the stream handle, and 10 % of the atoms given a type
+    outside [0, n_types): those atoms take no part, the rest match the NumPy restatement."""
+    import torch
+    lib = _lib()
+    f = lib.mdelast_pair_correlation_static
+    case = dynamics_case(nside=5, n_zn=30, ensemble=1)
+    d = gpu(case)
+    for _ in range(4):
+        d.integrate()
+    crd_h = gpu_atoms(d, "coordinates")
+    nt = len(case.tables.masses)
+    types = np.asarray(case.types, dtype=np.uint32).copy()
+    rs = np.random.RandomState(5)
+    types[rs.choice(len(types), size=len(types) // 10, replace=False)] = nt + 3
+    h = np.diag(np.asarray(d.box.h)).copy()
+    rg_h = np.asarray(d.rg, dtype=float)
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        crd = torch.tensor(crd_h, dtype=torch.float64, device="cuda")
+        typ = torch.tensor(types.astype(np.int32), device="cuda")
+        rg = torch.tensor(rg_h, dtype=torch.float64, device="cuda")
+        npair = nt * (nt + 1) // 2
+        box = (C.c_double * 3)(*h)
+        for call in range(2):
+            g = torch.full((len(rg_h),), -1.0, dtype=torch.float64, device="cuda")
+            gp = torch.full((npair, len(rg_h)), -1.0, dtype=torch.float64, device="cuda")
+            rc = f(crd.data_ptr(), typ.data_ptr(), len(types), nt, box, rg.data_ptr(),
+                   len(rg_h), 1, g.data_ptr(), gp.data_ptr(), C.c_void_p(side.cuda_stream))
+            assert rc == 0, lib.mdelast_last_error().decode()
+            side.synchronize()
+            g_np, gp_np = numpy_gr(crd_h, types, nt, h, rg_h, 1)
+            assert np.abs(g.cpu().numpy() - g_np).max() <= 1e-12 * np.abs(g_np).max()
+            assert np.abs(gp.cpu().numpy() - gp_np).max() <= 1e-12 * np.abs(gp_np).max()
+            assert g_np.sum() > 0 and gp_np.sum() > 0
 
 
 @pytest.mark.gpu
