@@ -281,15 +281,28 @@ int mdelast_batch_get_gr(mdelast_driver *d, int32_t replica, double *gr, double 
  * serial). autotune times the density and the force pass (sampled-step variants when the
  * driver samples observables, else the plain ones) on the current positions for every
  * lanes-per-atom value in {1, 4, 8, 16} and block target in {8, 16, 32, 64} x 148, n_repeat
- * launches each, keeps the fastest for each pass and recomputes the per-atom state with it;
- * the state does not advance. choice (4 values, may be NULL): lanes per atom of the density
- * and force passes, block targets of the density and force passes; ms_out (2, may be NULL):
- * their mean times in ms. set_launch sets a shape directly. Both drop the captured step
- * graphs (recaptured on the next step). */
+ * launches each, and where the tables are staged (below) also the staged force pass with
+ * 4, 8 or 16 lanes per atom and {1, 2, 4} x 148 blocks of 512 threads; it keeps the fastest
+ * for each pass and recomputes the per-atom state with it; the state does not advance.
+ * choice (4 values, may be NULL): lanes per atom of the density and force passes, block
+ * targets of the density and force passes; ms_out (2, may be NULL): their mean times in
+ * ms. set_launch sets a shape directly (keeping the force-pass variant). Both drop the
+ * captured step graphs (recaptured on the next step). */
 int mdelast_driver_autotune(mdelast_driver *d, int32_t n_repeat, int32_t *choice,
                             double *ms_out);
 int mdelast_driver_set_launch(mdelast_driver *d, int32_t tpa_density, int32_t tpa_force,
                               int32_t blocks_density, int32_t blocks_force);
+/* The staged force pass. No counterpart in the reference. In mixed precision with quintic
+ * EAM tables, a driver keeps an FP32 copy of the top intervals of every phi_ab and rho_a
+ * (those up to the largest cutoff, at most 184 KB; each function once), and the staged
+ * force pass copies it into each block's shared memory and reads the tables there instead
+ * of through the L1 (a two-element alloy's tables fit down to r of about 1.6 A; shorter
+ * pairs read the global tables). Per-atom results are bit for bit those of the other
+ * force pass. set: on (1) or off (0), with the current lanes per atom (4, 8 or 16 when on)
+ * and block target; MDELAST_ERR_UNSUPPORTED when no staged copy exists. get: *on the
+ * variant in use, *available whether a staged copy exists (either may be NULL). */
+int mdelast_driver_set_force_staging(mdelast_driver *d, int32_t on);
+int mdelast_driver_get_force_staging(mdelast_driver *d, int32_t *on, int32_t *available);
 /* The list the pair passes walk. No counterpart in the reference (its passes walk the
  * neighbour list, whose pairs beyond r_cut they skip). factor > 1: the neighbour list's
  * pairs within factor * r_cut (FP64 min-image, the same test from both atoms), rebuilt after

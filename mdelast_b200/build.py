@@ -52,7 +52,7 @@ def build_cuda_library(verbose_ptxas=False):
     srcs = [os.path.join(CSRC, f) for f in CUDA_SOURCES + HOST_SOURCES]
     if not _stale(out, srcs + headers) and not verbose_ptxas:
         return out
-    objs = []
+    objs, cmds = [], []
     obj_dir = os.path.join(HERE, "_build")
     os.makedirs(obj_dir, exist_ok=True)
     for f in CUDA_SOURCES:
@@ -61,13 +61,18 @@ def build_cuda_library(verbose_ptxas=False):
                "-I" + INCLUDE, "-I" + CSRC, "-c", os.path.join(CSRC, f), "-o", o]
         if verbose_ptxas:
             cmd.insert(1, "-Xptxas=-v")
-        _run(cmd)
+        cmds.append(cmd)
         objs.append(o)
     for f in HOST_SOURCES:
         o = os.path.join(obj_dir, f + ".o")
-        _run(["g++", "-std=c++17", "-O2", "-fPIC", "-Wall", "-Wextra", "-I" + INCLUDE,
-              "-I" + CSRC, "-c", os.path.join(CSRC, f), "-o", o])
+        cmds.append(["g++", "-std=c++17", "-O2", "-fPIC", "-Wall", "-Wextra", "-I" + INCLUDE,
+                     "-I" + CSRC, "-c", os.path.join(CSRC, f), "-o", o])
         objs.append(o)
+    # the translation units are independent: compile them side by side
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as pool:
+        for f in [pool.submit(_run, c) for c in cmds]:
+            f.result()
     _run([NVCC, *ARCH, "-shared", "-o", out, *objs, "-lcudart"])
     return out
 

@@ -359,7 +359,7 @@ __global__ void k_nbr_build(AtomsView A, int cells_done) {
 // so those per-atom Born and Laplacian terms (md_driver.cpp:410-419) are formed here and
 // g, h are never stored.
 
-template <bool OBS, int TPA, int IP>
+template <bool OBS, int TPA, int IP, typename IX>
 __global__ void __launch_bounds__(kBlock) k_density(AtomsView A, TablesView T) {
     constexpr int kF = TabFmt<IP>::kF;
     int const r = A.dblk_rep[blockIdx.x];
@@ -383,13 +383,13 @@ __global__ void __launch_bounds__(kBlock) k_density(AtomsView A, TablesView T) {
         ci = A.crd[i];
         int const ti = static_cast<int>(ci.w);
         int const nu = A.pn_up[i], ntot = nu + A.pn_dn[i];
-        int const *row = A.pnbr + static_cast<size_t>(i) * A.pmaxn;
+        PairRow<IX> const row = pair_row<IX>(A, i, R->atom_begin);
         // the next partner's index and record are loaded one iteration ahead
-        double4 cn = A.crd[sub < ntot ? row[list_slot(sub, nu, A.pmaxn)] : i];
+        double4 cn = A.crd[sub < ntot ? row.at(list_slot(sub, nu, A.pmaxn)) : i];
         for (int kk = sub; kk < ntot; kk += TPA) {
             double4 const cj = cn;
             if (kk + TPA < ntot)
-                cn = A.crd[row[list_slot(kk + TPA, nu, A.pmaxn)]];
+                cn = A.crd[row.at(list_slot(kk + TPA, nu, A.pmaxn))];
             double px, py, pz;
             double const r2 = min_image_r2(ci, cj, hx, hy, hz, px, py, pz);
             if (r2 > T.r_cut_sq)
@@ -470,7 +470,7 @@ __global__ void __launch_bounds__(kBlock) k_density(AtomsView A, TablesView T) {
 // its j > i visit; the Born tensor is accumulated as the 15 distinct degree-4 monomials
 // X p_a p_b p_c p_d of which its 21 upper-triangle entries are made.
 
-template <bool OBS, bool KICK, int TPA, int IP>
+template <bool OBS, bool KICK, int TPA, int IP, typename IX>
 __global__ void __launch_bounds__(kBlock) k_force(AtomsView A, TablesView T) {
     constexpr int kF = TabFmt<IP>::kF;
     int const r = A.fblk_rep[blockIdx.x];
@@ -495,10 +495,10 @@ __global__ void __launch_bounds__(kBlock) k_force(AtomsView A, TablesView T) {
         double2 const dFi2 = T.has_eam ? A.dF2[i] : make_double2(0., 0.);
         double const dFi = dFi2.x, d2Fi = OBS ? dFi2.y : 0.;
         int const nu = A.pn_up[i], ntot = nu + A.pn_dn[i];
-        int const *row = A.pnbr + static_cast<size_t>(i) * A.pmaxn;
+        PairRow<IX> const row = pair_row<IX>(A, i, R->atom_begin);
         bool warn_rmin = false;
         // the next partner's index, record and F' are loaded one iteration ahead
-        int jn = sub < ntot ? row[list_slot(sub, nu, A.pmaxn)] : i;
+        int jn = sub < ntot ? row.at(list_slot(sub, nu, A.pmaxn)) : i;
         double4 cn = A.crd[jn];
         double2 fn = A.dF2[jn];
         for (int kk = sub; kk < ntot; kk += TPA) {
@@ -506,7 +506,7 @@ __global__ void __launch_bounds__(kBlock) k_force(AtomsView A, TablesView T) {
             double4 const cj = cn;
             double2 const dFj2 = fn;
             if (kk + TPA < ntot) {
-                jn = row[list_slot(kk + TPA, nu, A.pmaxn)];
+                jn = row.at(list_slot(kk + TPA, nu, A.pmaxn));
                 cn = A.crd[jn];
                 fn = A.dF2[jn];
             }
@@ -718,6 +718,14 @@ __device__ __forceinline__ void sublist_row(AtomsView const &A, int i, int lane)
     int const nu = A.n_up[i], nd = A.n_dn[i];
     int const *row = A.nbr + static_cast<size_t>(i) * A.maxn;
     int *out = A.pnbr + static_cast<size_t>(i) * A.pmaxn;
+    uint16_t *out16 = A.pnbr16 ? A.pnbr16 + static_cast<size_t>(i) * A.pmaxn : nullptr;
+    int const base = R->atom_begin;
+    auto put = [&](int slot, int j) {
+        if (out16)
+            out16[slot] = static_cast<uint16_t>(j - base);
+        else
+            out[slot] = j;
+    };
     unsigned const lt = (1u << lane) - 1u;
     int ku = 0, kd = 0;
     for (int k0 = 0; k0 < nu + nd; k0 += 32) {
@@ -732,9 +740,9 @@ __device__ __forceinline__ void sublist_row(AtomsView const &A, int i, int lane)
         unsigned const bu = __ballot_sync(0xffffffffu, keep && upper);
         unsigned const bd = __ballot_sync(0xffffffffu, keep && !upper);
         if (keep && upper)
-            out[ku + __popc(bu & lt)] = j;
+            put(ku + __popc(bu & lt), j);
         if (keep && !upper)
-            out[A.pmaxn - 1 - (kd + __popc(bd & lt))] = j;
+            put(A.pmaxn - 1 - (kd + __popc(bd & lt)), j);
         ku += __popc(bu);
         kd += __popc(bd);
     }
@@ -913,23 +921,37 @@ __global__ void k_table_eval(TablesView T, int which, int s, const double *x, in
 }
 
 namespace {
+template <bool OBS, int IP, typename IX>
+void density_tpa_ix(int tpa, int grid, cudaStream_t s, AtomsView const &A, TablesView const &T) {
+    switch (tpa) {
+    case 1: k_density<OBS, 1, IP, IX><<<grid, kBlock, 0, s>>>(A, T); break;
+    case 4: k_density<OBS, 4, IP, IX><<<grid, kBlock, 0, s>>>(A, T); break;
+    case 8: k_density<OBS, 8, IP, IX><<<grid, kBlock, 0, s>>>(A, T); break;
+    default: k_density<OBS, 16, IP, IX><<<grid, kBlock, 0, s>>>(A, T); break;
+    }
+}
 template <bool OBS, int IP>
 void density_tpa(int tpa, int grid, cudaStream_t s, AtomsView const &A, TablesView const &T) {
+    if (A.pnbr16)
+        density_tpa_ix<OBS, IP, uint16_t>(tpa, grid, s, A, T);
+    else
+        density_tpa_ix<OBS, IP, int>(tpa, grid, s, A, T);
+}
+template <bool OBS, bool KICK, int IP, typename IX>
+void force_tpa_ix(int tpa, int grid, cudaStream_t s, AtomsView const &A, TablesView const &T) {
     switch (tpa) {
-    case 1: k_density<OBS, 1, IP><<<grid, kBlock, 0, s>>>(A, T); break;
-    case 4: k_density<OBS, 4, IP><<<grid, kBlock, 0, s>>>(A, T); break;
-    case 8: k_density<OBS, 8, IP><<<grid, kBlock, 0, s>>>(A, T); break;
-    default: k_density<OBS, 16, IP><<<grid, kBlock, 0, s>>>(A, T); break;
+    case 1: k_force<OBS, KICK, 1, IP, IX><<<grid, kBlock, 0, s>>>(A, T); break;
+    case 4: k_force<OBS, KICK, 4, IP, IX><<<grid, kBlock, 0, s>>>(A, T); break;
+    case 8: k_force<OBS, KICK, 8, IP, IX><<<grid, kBlock, 0, s>>>(A, T); break;
+    default: k_force<OBS, KICK, 16, IP, IX><<<grid, kBlock, 0, s>>>(A, T); break;
     }
 }
 template <bool OBS, bool KICK, int IP>
 void force_tpa(int tpa, int grid, cudaStream_t s, AtomsView const &A, TablesView const &T) {
-    switch (tpa) {
-    case 1: k_force<OBS, KICK, 1, IP><<<grid, kBlock, 0, s>>>(A, T); break;
-    case 4: k_force<OBS, KICK, 4, IP><<<grid, kBlock, 0, s>>>(A, T); break;
-    case 8: k_force<OBS, KICK, 8, IP><<<grid, kBlock, 0, s>>>(A, T); break;
-    default: k_force<OBS, KICK, 16, IP><<<grid, kBlock, 0, s>>>(A, T); break;
-    }
+    if (A.pnbr16)
+        force_tpa_ix<OBS, KICK, IP, uint16_t>(tpa, grid, s, A, T);
+    else
+        force_tpa_ix<OBS, KICK, IP, int>(tpa, grid, s, A, T);
 }
 template <int IP>
 void density_ip(bool obs, int tpa, int grid, cudaStream_t s, AtomsView const &A,

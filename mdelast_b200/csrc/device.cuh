@@ -107,6 +107,12 @@ struct TablesView {
     // Cutoffs in angstrom.
     const float *rbf, *rrf;
     float finv_hr, finv_hr2, fr_cut_sq, fpad;
+    // Staged copy for the shared-memory force pass (quintic only): the intervals
+    // [st_lo, st_lo + st_n) of every phi_ab (slot s at s * st_n) followed by every rho_a
+    // (type a at (npot + a) * st_n), 6 floats each, de-duplicated (each rho once, not once
+    // per type pair). st_n == 0: no staged copy. st_bytes: its size (a multiple of 16).
+    const float *stf;
+    int st_lo, st_n, st_bytes, st_pad;
     float fpot_rcut[kMaxTypes * (kMaxTypes + 1) / 2];
     float fpot_rmin[kMaxTypes * (kMaxTypes + 1) / 2];
     float feam_rcut[kMaxTypes];
@@ -143,7 +149,11 @@ struct AtomsView {
     // The list the pair passes read: the neighbour list itself, or its pairs within
     // sub_r2 (squared radius, cm^2) kept since the coordinates crd_ref; refreshed once some
     // atom has moved by more than half the radius margin (sub_half2 = that half, squared).
+    // pnbr16 (when not null) holds the pair list instead of pnbr, each entry the partner's
+    // offset from its replica's first slot in 16 bits (replicas of at most 65,536 atoms):
+    // half the bytes the pair passes read per pair.
     int *pnbr, *pn_up, *pn_dn;
+    uint16_t *pnbr16;
     int pmaxn, pad_p;
     double4 *crd_ref;     // null: the pair passes read the neighbour list
     double sub_r2, sub_half2;
@@ -167,6 +177,30 @@ __device__ __forceinline__ double min_image_r2(double4 ci, double4 cj, double hx
     py = __dmul_rn(dy, hy);
     pz = __dmul_rn(dz, hz);
     return __dadd_rn(__dadd_rn(__dmul_rn(px, px), __dmul_rn(py, py)), __dmul_rn(pz, pz));
+}
+
+// Row i of the pair list in either entry width: at(k) is the atom slot of list slot k
+// (partners j > i from slot 0 up, j < i from slot pmaxn - 1 down). IX = int: slots as stored;
+// IX = uint16_t: offsets from the replica's first slot `base`. Loads stream (evict first):
+// each row is read once per pass.
+template <typename IX> struct PairRow {
+    const IX *p;
+    int base;
+    __device__ __forceinline__ int at(int k) const {
+        if constexpr (sizeof(IX) == 2)
+            return base + static_cast<int>(__ldcs(p + k));
+        else
+            return __ldcs(p + k);
+    }
+};
+template <typename IX>
+__device__ __forceinline__ PairRow<IX> pair_row(AtomsView const &A, int i, int base) {
+    const IX *p;
+    if constexpr (sizeof(IX) == 2)
+        p = A.pnbr16;
+    else
+        p = A.pnbr;
+    return PairRow<IX>{p + static_cast<size_t>(i) * A.pmaxn, base};
 }
 
 __host__ __device__ __forceinline__ int pair_slot(int a, int b) {

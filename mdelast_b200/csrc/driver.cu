@@ -108,19 +108,25 @@ int default_tpa(int n_atoms) {
 // atom group of kBlock/tpa atoms. Fills each replica's block range and the block ->
 // replica map; returns the grid size.
 constexpr int kTargetBlocks = 148 * 32;
+// shared memory for the staged force tables: beside it the kernel keeps its FP64
+// accumulators (40 KB at 4 lanes per atom) within the 227 KB a block may take
+constexpr long kStageBudget = 184 * 1024;
 // k_sublist grid: one wave, 4 resident blocks of 256 threads (48 registers each) on each of
 // the 148 SMs
 constexpr int kSublistBlocks = 148 * 4;
 
 int deal_blocks(std::vector<Replica *> const &reps, int tpa, bool density,
-                std::vector<int> &blk_rep, int target = kTargetBlocks) {
+                std::vector<int> &blk_rep, int target = kTargetBlocks,
+                int block_threads = kBlock) {
     long total = 0;
     for (Replica const *r : reps)
         total += r->n_blocks;
     blk_rep.clear();
     for (size_t k = 0; k < reps.size(); ++k) {
         Replica *r = reps[k];
-        long const most = static_cast<long>(r->n_blocks) * tpa;
+        // atom groups of block_threads / tpa atoms in the replica's kBlock-multiple range
+        long const most = (static_cast<long>(r->n_blocks) * kBlock * tpa + block_threads - 1) /
+                          block_threads;
         long nb = (static_cast<long>(target) * r->n_blocks + total - 1) / total;
         nb = std::max(1L, std::min(nb, most));
         if (density) {
@@ -184,8 +190,17 @@ struct mdelast_driver_s {
         else
             launch_density(obs, tpa_d, grid_d, s, A, T);
     }
+    // force pass with the staged shared-memory tables (mixed precision, quintic, when the
+    // tables were staged; chosen by the autotuner or set_force_staging)
+    bool stage_f = false;
+    float *d_stf = nullptr;
+    bool staging_available() const {
+        return precision == MDELAST_PRECISION_MIXED && T.st_n > 0;
+    }
     void pass_force(bool obs, bool kick, cudaStream_t s) {
-        if (precision == MDELAST_PRECISION_MIXED)
+        if (precision == MDELAST_PRECISION_MIXED && stage_f && T.st_n > 0)
+            launch_force_mx_staged(obs, kick, tpa_f, grid_f, s, A, T);
+        else if (precision == MDELAST_PRECISION_MIXED)
             launch_force_mx(obs, kick, tpa_f, grid_f, s, A, T);
         else
             launch_force(obs, kick, tpa_f, grid_f, s, A, T);
@@ -193,6 +208,11 @@ struct mdelast_driver_s {
     int *d_nbr = nullptr, *d_nup = nullptr, *d_ndn = nullptr;
     // pair list of the pair passes (see AtomsView::pnbr); pair_factor 0: the neighbour list
     int *d_pnbr = nullptr, *d_pnup = nullptr, *d_pndn = nullptr;
+    // 16-bit entries (offsets within the replica) when every replica has at most 65,536
+    // atoms; MDELAST_PAIR_LIST_16=0 keeps 32-bit entries
+    uint16_t *d_pnbr16 = nullptr;
+    bool pair16 = false;
+    int alloc_pair_rows();
     double4 *d_crd_ref = nullptr;
     double pair_factor = 0., rcut0 = 0.;
     int set_pair_list(double factor);
@@ -255,7 +275,7 @@ struct mdelast_driver_s {
     int check_status();
     // launch shape of the pair passes: lanes per atom and target block counts
     int target_d = kTargetBlocks, target_f = kTargetBlocks;
-    int set_launch(int tpa_d_, int tpa_f_, int tgt_d, int tgt_f);
+    int set_launch(int tpa_d_, int tpa_f_, int tgt_d, int tgt_f, int staged = -1);
     int time_passes(int n_repeat, int obs, double *ms_d, double *ms_f);
 };
 
@@ -282,10 +302,12 @@ mdelast_driver_s::~mdelast_driver_s() {
     dfree(d_dF2f);
     dfree(d_rbf);
     dfree(d_rrf);
+    dfree(d_stf);
     dfree(d_nbr);
     dfree(d_nup);
     dfree(d_ndn);
     dfree(d_pnbr);
+    dfree(d_pnbr16);
     dfree(d_pnup);
     dfree(d_pndn);
     dfree(d_crd_ref);
@@ -319,19 +341,27 @@ int mdelast_driver_s::alloc_list(int maxn) {
         return rc;
     A.nbr = d_nbr;
     A.maxn = maxn;
-    if (pair_factor > 0.) {
-        dfree(d_pnbr);
-        if (int rc = dalloc(&d_pnbr, static_cast<size_t>(maxn) * n_pad))
+    if (pair_factor > 0.)
+        if (int rc = alloc_pair_rows())
             return rc;
-    }
     point_pair_list();
     drop_graphs();
     return MDELAST_OK;
 }
 
+// rows of the pair list at the neighbour list's capacity, in the chosen entry width
+int mdelast_driver_s::alloc_pair_rows() {
+    dfree(d_pnbr);
+    dfree(d_pnbr16);
+    size_t const n = static_cast<size_t>(A.maxn) * n_pad;
+    return pair16 ? dalloc(&d_pnbr16, n) : dalloc(&d_pnbr, n);
+}
+
 void mdelast_driver_s::point_pair_list() {
+    A.pnbr16 = nullptr;
     if (pair_factor > 0.) {
         A.pnbr = d_pnbr;
+        A.pnbr16 = pair16 ? d_pnbr16 : nullptr;
         A.pn_up = d_pnup;
         A.pn_dn = d_pndn;
         A.crd_ref = d_crd_ref;
@@ -358,12 +388,20 @@ int mdelast_driver_s::set_pair_list(double factor) {
     CK(cudaStreamSynchronize(stream));
     drop_graphs();
     dfree(d_pnbr);
+    dfree(d_pnbr16);
     dfree(d_pnup);
     dfree(d_pndn);
     dfree(d_crd_ref);
     pair_factor = factor;
+    {
+        int most = 0;
+        for (int c : rep_count)
+            most = std::max(most, c);
+        char const *e = std::getenv("MDELAST_PAIR_LIST_16");
+        pair16 = most <= 65536 && !(e && std::atoi(e) == 0);
+    }
     if (factor > 0.) {
-        if (int rc = dalloc(&d_pnbr, static_cast<size_t>(A.maxn) * n_pad))
+        if (int rc = alloc_pair_rows())
             return rc;
         if (int rc = dalloc(&d_pnup, static_cast<size_t>(n_pad)))
             return rc;
@@ -405,9 +443,15 @@ int mdelast_driver_s::alloc_cells(int n_cells, int cell_cap) {
 // Re-deal the pair-pass blocks for new lanes-per-atom and block targets: replica block
 // ranges, block -> replica maps, per-block and per-chunk partial-sum buffers. The step
 // graphs hold the old shapes and are dropped. Call with no work in flight.
-int mdelast_driver_s::set_launch(int tpa_d_, int tpa_f_, int tgt_d, int tgt_f) {
+int mdelast_driver_s::set_launch(int tpa_d_, int tpa_f_, int tgt_d, int tgt_f, int staged) {
     if (!valid_tpa(tpa_d_) || !valid_tpa(tpa_f_) || tgt_d < 1 || tgt_f < 1)
         return fail(MDELAST_ERR_ARGUMENT, "bad launch shape");
+    bool const st = staged < 0 ? stage_f : staged != 0;
+    if (st && !staging_available())
+        return fail(MDELAST_ERR_UNSUPPORTED,
+                    "staged force tables need mixed precision and quintic tables that fit");
+    if (st && tpa_f_ == 1)
+        return fail(MDELAST_ERR_ARGUMENT, "the staged force pass takes 4, 8 or 16 lanes per atom");
     CK(cudaStreamSynchronize(stream));
     std::vector<Replica> R(static_cast<size_t>(n_rep));
     CK(cudaMemcpy(R.data(), d_rep, sizeof(Replica) * n_rep, cudaMemcpyDeviceToHost));
@@ -416,7 +460,7 @@ int mdelast_driver_s::set_launch(int tpa_d_, int tpa_f_, int tgt_d, int tgt_f) {
         reps.push_back(&x);
     std::vector<int> dmap, fmap;
     int const gd = deal_blocks(reps, tpa_d_, true, dmap, tgt_d);
-    int const gf = deal_blocks(reps, tpa_f_, false, fmap, tgt_f);
+    int const gf = deal_blocks(reps, tpa_f_, false, fmap, tgt_f, st ? kStagedBlock : kBlock);
     int chunks = 1;
     for (Replica const *x : reps)
         chunks = std::max(chunks, (std::max(x->dblk_n, x->fblk_n) + kChunk - 1) / kChunk);
@@ -450,6 +494,7 @@ int mdelast_driver_s::set_launch(int tpa_d_, int tpa_f_, int tgt_d, int tgt_f) {
     tpa_f = tpa_f_;
     target_d = tgt_d;
     target_f = tgt_f;
+    stage_f = st;
     grid_d = gd;
     grid_f = gf;
     A.dblk_rep = d_dblk_rep;
@@ -1026,6 +1071,46 @@ static int create_system(const mdelast_driver_config *cfgs, int n_rep, mdelast_d
             return bail(fail(MDELAST_ERR_CUDA, "table upload failed"));
         T.rbf = d->d_rbf;
         T.rrf = d->d_rrf;
+        // The staged copy of the force pass: every phi_ab, then every rho_a, over the top
+        // intervals of the r grid (those below r_cut, as many as kStageBudget holds), the
+        // same FP32 values as the bundles. Quintic EAM tables only.
+        if (!bsp && c0.n_eam) {
+            int const n_fun = npot + nt;
+            double rc_max = 0.;
+            for (int q = 0; q < npot; ++q)
+                rc_max = std::max(rc_max, T.pot_rcut[q]);
+            for (int q = 0; q < nt; ++q)
+                rc_max = std::max(rc_max, T.eam_rcut[q]);
+            long const k_hi = std::min<long>(
+                nri, static_cast<long>(std::floor(rc_max / kAng * (T.inv_hr * kAng))) + 2);
+            long const fit = kStageBudget / (static_cast<long>(n_fun) * 24);
+            long const n_st = std::min(k_hi, fit);
+            if (n_st >= 16) {
+                long const lo = k_hi - n_st;
+                size_t const nfl = static_cast<size_t>(n_fun) * n_st * 6;
+                std::vector<float> stf((nfl + 3) / 4 * 4, 0.f);
+                for (int q = 0; q < n_fun; ++q)
+                    for (long k = 0; k < n_st; ++k) {
+                        float *o = stf.data() + (static_cast<size_t>(q) * n_st + k) * 6;
+                        if (q < npot)
+                            pack(fun(c0.pair[q]->table, static_cast<int>(lo + k)), 1. / kEv, o);
+                        else
+                            pack(fun(c0.eam[q - npot]->rho, static_cast<int>(lo + k)), a3, o);
+                    }
+                TRY(dalloc(&d->d_stf, stf.size()));
+                if (cudaMemcpy(d->d_stf, stf.data(), sizeof(float) * stf.size(),
+                               cudaMemcpyHostToDevice))
+                    return bail(fail(MDELAST_ERR_CUDA, "table upload failed"));
+                T.stf = d->d_stf;
+                T.st_lo = static_cast<int>(lo);
+                T.st_n = static_cast<int>(n_st);
+                T.st_bytes = static_cast<int>(sizeof(float) * stf.size());
+                // the kernels' limit is the budget, not this copy's size: another driver
+                // in the process may stage a larger copy
+                if (cudaError_t e = prepare_force_mx_staged(static_cast<int>(kStageBudget)))
+                    return bail(fail(MDELAST_ERR_CUDA, "staged kernels: %s", cudaGetErrorString(e)));
+            }
+        }
         T.finv_hr = static_cast<float>(T.inv_hr * kAng);
         T.finv_hr2 = static_cast<float>(T.inv_hr2 * kAng * kAng);
         T.fr_cut_sq = static_cast<float>((rcut / kAng) * (rcut / kAng));
@@ -1601,10 +1686,10 @@ int mdelast_driver_autotune(mdelast_driver *d, int32_t n_repeat, int32_t *choice
     int const tpas[4] = {1, 4, 8, 16};
     int const targets[4] = {148 * 8, 148 * 16, 148 * 32, 148 * 64};
     double best_d = 1e300, best_f = 1e300;
-    int bd[2] = {d->tpa_d, d->target_d}, bf[2] = {d->tpa_f, d->target_f};
+    int bd[2] = {d->tpa_d, d->target_d}, bf[3] = {d->tpa_f, d->target_f, d->stage_f ? 1 : 0};
     for (int tp : tpas)
         for (int tg : targets) {
-            if (int rc = d->set_launch(tp, tp, tg, tg))
+            if (int rc = d->set_launch(tp, tp, tg, tg, 0))
                 return rc;
             double md = 0., mf = 0.;
             if (int rc = d->time_passes(n_repeat, d->sample, &md, &mf))
@@ -1618,9 +1703,26 @@ int mdelast_driver_autotune(mdelast_driver *d, int32_t n_repeat, int32_t *choice
                 best_f = mf;
                 bf[0] = tp;
                 bf[1] = tg;
+                bf[2] = 0;
             }
         }
-    if (int rc = d->set_launch(bd[0], bf[0], bd[1], bf[1]))
+    // the staged force pass: one 512-thread block per SM, one to four waves
+    if (d->staging_available())
+        for (int tp : {4, 8, 16})
+            for (int tg : {148, 148 * 2, 148 * 4}) {
+                if (int rc = d->set_launch(bd[0], tp, bd[1], tg, 1))
+                    return rc;
+                double md = 0., mf = 0.;
+                if (int rc = d->time_passes(n_repeat, d->sample, &md, &mf))
+                    return rc;
+                if (mf < best_f) {
+                    best_f = mf;
+                    bf[0] = tp;
+                    bf[1] = tg;
+                    bf[2] = 1;
+                }
+            }
+    if (int rc = d->set_launch(bd[0], bf[0], bd[1], bf[1], bf[2]))
         return rc;
     // recompute the per-atom state with the chosen shapes (positions are unchanged)
     double md = 0., mf = 0.;
@@ -1651,6 +1753,30 @@ int mdelast_driver_set_launch(mdelast_driver *d, int32_t tpa_density, int32_t tp
         return rc;
     double md = 0., mf = 0.;
     return d->time_passes(1, 1, &md, &mf);
+}
+
+int mdelast_driver_set_force_staging(mdelast_driver *d, int32_t on) {
+    clear_error();
+    if (!d)
+        return fail(MDELAST_ERR_ARGUMENT, "null driver");
+    CK(cudaSetDevice(d->device));
+    if (int rc = d->wait_step())
+        return rc;
+    if (int rc = d->set_launch(d->tpa_d, d->tpa_f, d->target_d, d->target_f, on ? 1 : 0))
+        return rc;
+    double md = 0., mf = 0.;
+    return d->time_passes(1, 1, &md, &mf);
+}
+
+int mdelast_driver_get_force_staging(mdelast_driver *d, int32_t *on, int32_t *available) {
+    clear_error();
+    if (!d)
+        return fail(MDELAST_ERR_ARGUMENT, "null driver");
+    if (on)
+        *on = d->stage_f ? 1 : 0;
+    if (available)
+        *available = d->staging_available() ? 1 : 0;
+    return MDELAST_OK;
 }
 
 int mdelast_driver_set_pair_list(mdelast_driver *d, double factor) {

@@ -25,6 +25,13 @@ void launch_density_mx(bool obs, int tpa, int grid, cudaStream_t s, AtomsView co
                        TablesView const &T);
 void launch_force_mx(bool obs, bool kick, int tpa, int grid, cudaStream_t s, AtomsView const &A,
                      TablesView const &T);
+// the mixed force pass with the quintic tables staged in shared memory (T.st_n > 0; tpa 4,
+// 8 or 16; blocks of kStagedBlock threads); prepare_force_mx_staged raises the kernels'
+// dynamic shared-memory limit (to the staging budget) before any launch or capture
+constexpr int kStagedBlock = 512;
+void launch_force_mx_staged(bool obs, bool kick, int tpa, int grid, cudaStream_t s,
+                            AtomsView const &A, TablesView const &T);
+cudaError_t prepare_force_mx_staged(int smem_bytes);
 __global__ void k_posf(AtomsView A);
 __global__ void k_kick_drift(AtomsView A, TablesView T);
 __global__ void k_pre(AtomsView A);

@@ -151,7 +151,19 @@ py::dict autotune_dict(mdelast_driver *d, int n_repeat) {
     out["blocks_force"] = c[3];
     out["ms_density"] = ms[0];
     out["ms_force"] = ms[1];
+    int32_t on = 0;
+    check(mdelast_driver_get_force_staging(d, &on, nullptr));
+    out["force_staged"] = on != 0;
     return out;
+}
+
+// the force-pass variant with the tables staged in shared memory (read / switch)
+py::object force_staging_get(mdelast_driver *d) {
+    int32_t on = 0, avail = 0;
+    check(mdelast_driver_get_force_staging(d, &on, &avail));
+    if (!avail)
+        return py::none();
+    return py::bool_(on != 0);
 }
 
 int parse_interp(std::string const &name) {
@@ -546,6 +558,8 @@ class MDDriver {
     void synchronize() { check(mdelast_driver_synchronize(d_)); }
     void set_sample_ring(int capacity) { check(mdelast_driver_set_sample_ring(d_, capacity)); }
     py::dict autotune(int n_repeat) { return autotune_dict(d_, n_repeat); }
+    py::object force_staging() { return force_staging_get(d_); }
+    void set_force_staging(bool on) { check(mdelast_driver_set_force_staging(d_, on ? 1 : 0)); }
     void set_launch(int td, int tf, int bd, int bf) {
         check(mdelast_driver_set_launch(d_, td, tf, bd, bf));
     }
@@ -838,6 +852,8 @@ class BatchedMDDriver {
     // returns (gr, gr_partial) with gr_partial one row per type pair a <= b
     void set_sample_ring(int capacity) { check(mdelast_driver_set_sample_ring(d_, capacity)); }
     py::dict autotune(int n_repeat) { return autotune_dict(d_, n_repeat); }
+    py::object force_staging() { return force_staging_get(d_); }
+    void set_force_staging(bool on) { check(mdelast_driver_set_force_staging(d_, on ? 1 : 0)); }
     void set_launch(int td, int tf, int bd, int bf) {
         check(mdelast_driver_set_launch(d_, td, tf, bd, bf));
     }
@@ -1024,6 +1040,8 @@ PYBIND11_MODULE(md_driver_module, m) {
              "time the pair passes over their launch shapes and keep the fastest")
         .def("set_launch", &MDDriver::set_launch, py::arg("tpa_density"), py::arg("tpa_force"),
              py::arg("blocks_density"), py::arg("blocks_force"))
+        .def_property("force_staging", &MDDriver::force_staging, &MDDriver::set_force_staging,
+                      "force pass reading shared-memory tables (None: no staged copy)")
         .def("set_pair_list", &MDDriver::set_pair_list, py::arg("factor"),
              "pair passes walk the list's pairs within factor * r_cut (0: the full list)")
         .def("set_sample_ring", &MDDriver::set_sample_ring, py::arg("capacity"),
@@ -1085,6 +1103,8 @@ PYBIND11_MODULE(md_driver_module, m) {
         .def("autotune", &BatchedMDDriver::autotune, py::arg("n_repeat") = 3)
         .def("set_launch", &BatchedMDDriver::set_launch, py::arg("tpa_density"),
              py::arg("tpa_force"), py::arg("blocks_density"), py::arg("blocks_force"))
+        .def_property("force_staging", &BatchedMDDriver::force_staging,
+                      &BatchedMDDriver::set_force_staging)
         .def("set_pair_list", &BatchedMDDriver::set_pair_list, py::arg("factor"))
         .def("set_sample_ring", &BatchedMDDriver::set_sample_ring, py::arg("capacity"))
         .def("drain_samples", &BatchedMDDriver::drain_samples, py::arg("replica"))

@@ -140,7 +140,7 @@ __device__ __forceinline__ void warp_accumulate(double v, double *slot) {
 // accumulators instead of being carried in registers through the pair loop: the loop then
 // runs with about half the registers, so twice the warps per SM hide the latency of the
 // partner gathers.
-template <bool OBS, int TPA, int IP>
+template <bool OBS, int TPA, int IP, typename IX>
 __global__ void __launch_bounds__(kBlock) k_density_mx(AtomsView A, TablesView T) {
     constexpr int kF = TabFmt<IP>::kF;
     __shared__ double sacc[kBlock / 32][D_NSUM];
@@ -167,12 +167,12 @@ __global__ void __launch_bounds__(kBlock) k_density_mx(AtomsView A, TablesView T
             float4 const pi = A.posf[i];
             ti = static_cast<int>(pi.w);
             int const nu = A.pn_up[i], ntot = nu + A.pn_dn[i];
-            int const *row = A.pnbr + static_cast<size_t>(i) * A.pmaxn;
-            float4 pn = A.posf[sub < ntot ? __ldcs(row + list_slot(sub, nu, A.pmaxn)) : i];
+            PairRow<IX> const row = pair_row<IX>(A, i, R->atom_begin);
+            float4 pn = A.posf[sub < ntot ? row.at(list_slot(sub, nu, A.pmaxn)) : i];
             for (int kk = sub; kk < ntot; kk += TPA) {
                 float4 const pj = pn;
                 if (kk + TPA < ntot)
-                    pn = A.posf[__ldcs(row + list_slot(kk + TPA, nu, A.pmaxn))];
+                    pn = A.posf[row.at(list_slot(kk + TPA, nu, A.pmaxn))];
                 float dx, dy, dz;
                 float const r2 = min_image_f(pi, pj, L, iL, dx, dy, dz);
                 if (r2 > T.fr_cut_sq)
@@ -289,35 +289,78 @@ struct RowIn {
     float3 L, iL;
 };
 
+// The quintic coefficients of phi_s, rho_ti and rho_tj on interval k: from the staged
+// shared-memory copy (STAGED and k staged) or from the global pair bundle. Both hold the
+// same FP32 values, so the pair terms do not depend on where they were read.
+template <bool STAGED>
+__device__ __forceinline__ void pair_coefs(TablesView const &T, const float *stab, int s,
+                                           int ti, int tj, int k, float cp[6], float ci[6],
+                                           float cj[6]) {
+    if (STAGED) {
+        unsigned const q = static_cast<unsigned>(k - T.st_lo);
+        if (q < static_cast<unsigned>(T.st_n)) {
+            int const n6 = 6 * T.st_n;
+            const float *b = stab + 6 * q;
+            const float2 *pp = reinterpret_cast<const float2 *>(b + s * n6);
+            const float2 *pi = reinterpret_cast<const float2 *>(b + (T.npot + ti) * n6);
+            const float2 *pj = reinterpret_cast<const float2 *>(b + (T.npot + tj) * n6);
+#pragma unroll
+            for (int u = 0; u < 3; ++u) {
+                float2 const a = pp[u], c = pi[u], d = pj[u];
+                cp[2 * u] = a.x;
+                cp[2 * u + 1] = a.y;
+                ci[2 * u] = c.x;
+                ci[2 * u + 1] = c.y;
+                cj[2 * u] = d.x;
+                cj[2 * u + 1] = d.y;
+            }
+            return;
+        }
+    }
+    constexpr int kFb = TabFmt<MDELAST_QUINTIC>::kFb;
+    const float *bundle = T.rbf + (static_cast<size_t>(s) * T.nri + k) * TabFmt<MDELAST_QUINTIC>::kB;
+    // rho_a of the bundle belongs to the smaller type of the pair
+    int const oi = (ti <= tj) ? kFb : 2 * kFb, oj = (ti < tj) ? 2 * kFb : kFb;
+    ld6f(bundle, cp);
+    ld6f(bundle + oi, ci);
+    ld6f(bundle + oj, cj);
+}
+
 // One lane's walk over list slots [s0, s1) of an atom row (slots of partners j > i when
 // UPPER, else of partners j < i, addressed from the end of the row); every pair adds its
 // force and half its energy to the atom, and pairs j > i also add to the global sums.
-template <bool OBS, bool UPPER, int TPA, int IP>
+// STAGED: quintic tables read from the staged shared-memory copy `stab` where staged.
+template <bool OBS, bool UPPER, int TPA, int IP, bool STAGED, typename IX>
 __device__ __forceinline__ void force_row_mx(AtomsView const &A, TablesView const &T,
-                                             RowIn const &in, const int *row, int n, int sub,
+                                             RowIn const &in, PairRow<IX> const &row, int n,
+                                             int sub,
                                              double &fx, double &fy, double &fz, double &epot,
-                                             PairSums<OBS> &ps, bool &warn_rmin) {
+                                             PairSums<OBS> &ps, bool &warn_rmin,
+                                             const float *stab = nullptr) {
     if (sub >= n)
         return;
     auto slot = [&](int k) { return UPPER ? k : A.pmaxn - 1 - k; };
     // the row's entries are read once per pass: streaming loads (evict first), so that
     // they do not push the table and the partner records out of the L1 (measured: step
     // 1.025 -> 0.987 ms at 16 x 13,500 atoms)
-    int jn = __ldcs(row + slot(sub));
+    int jn = row.at(slot(sub));
     float4 pn = A.posf[jn];
     float2 fn = A.dF2f[jn];
+    // The body has no branch: a pair beyond the cutoff is evaluated and its terms are
+    // replaced by zeros (the sums then gain +0 or -0, which changes no sum), and the next
+    // partner is always prefetched (the last one again at the end of the row). Two
+    // iterations then form one block of straight-line code, in which the second pair's
+    // gathers and table loads overlap the first pair's arithmetic.
+#pragma unroll 2
     for (int kk = sub; kk < n; kk += TPA) {
         float4 const pj = pn;
         float2 const dFj2 = fn;
-        if (kk + TPA < n) {
-            jn = __ldcs(row + slot(kk + TPA));
-            pn = A.posf[jn];
-            fn = A.dF2f[jn];
-        }
+        jn = row.at(slot(min(kk + TPA, n - 1)));
+        pn = A.posf[jn];
+        fn = A.dF2f[jn];
         float dx, dy, dz;
         float const r2 = min_image_f(in.pi, pj, in.L, in.iL, dx, dy, dz);
-        if (r2 > T.fr_cut_sq)
-            continue;
+        bool const in_cut = !(r2 > T.fr_cut_sq);
         float const idr = rsqrtf(r2);
         float const dr = __fmul_rn(r2, idr);
         int const tj = static_cast<int>(pj.w);
@@ -326,27 +369,52 @@ __device__ __forceinline__ void force_row_mx(AtomsView const &A, TablesView cons
         float t;
         int const k = tab_locate_f(dr, T.finv_hr, T.nri, t);
         constexpr int kFb = TabFmt<IP>::kFb;
-        const float *bundle = T.rbf + (static_cast<size_t>(s) * T.nri + k) * TabFmt<IP>::kB;
         float V = 0.f, dV = 0.f, d2V = 0.f;
-        if (dr < T.fpot_rmin[s])
+        float drho_i = 0.f, drho_j = 0.f, d2rho_i = 0.f, d2rho_j = 0.f;
+        if (in_cut && dr < T.fpot_rmin[s])
             warn_rmin = true;
-        if (!(dr > T.fpot_rcut[s]))
-            tabf_eval<IP, true, true, OBS>(bundle, t, T.finv_hr, T.finv_hr2, V, dV, d2V);
+        bool const eam_i = T.has_eam && !(dr > T.feam_rcut[ti]);
+        bool const eam_j = T.has_eam && !(dr > T.feam_rcut[tj]);
+        if constexpr (IP == MDELAST_QUINTIC) {
+            // the three functions' coefficients first (independent loads), then the math
+            float cp[6], ci[6], cj[6];
+            pair_coefs<STAGED>(T, stab, s, ti, tj, k, cp, ci, cj);
+            if (!(dr > T.fpot_rcut[s])) {
+                V = tabf_v(cp, t);
+                dV = tabf_d1(cp, t, T.finv_hr);
+                if (OBS)
+                    d2V = tabf_d2(cp, t, T.finv_hr2);
+            }
+            if (eam_i) {
+                drho_i = tabf_d1(ci, t, T.finv_hr);
+                if (OBS)
+                    d2rho_i = tabf_d2(ci, t, T.finv_hr2);
+            }
+            if (eam_j) {
+                drho_j = tabf_d1(cj, t, T.finv_hr);
+                if (OBS)
+                    d2rho_j = tabf_d2(cj, t, T.finv_hr2);
+            }
+        } else {
+            const float *bundle = T.rbf + (static_cast<size_t>(s) * T.nri + k) * TabFmt<IP>::kB;
+            if (!(dr > T.fpot_rcut[s]))
+                tabf_eval<IP, true, true, OBS>(bundle, t, T.finv_hr, T.finv_hr2, V, dV, d2V);
+            // rho'_{t_i} and rho'_{t_j} at r: rho_a of the bundle belongs to the smaller type
+            int const oi = (ti <= tj) ? kFb : 2 * kFb, oj = (ti < tj) ? 2 * kFb : kFb;
+            float unused = 0.f;
+            if (eam_i)
+                tabf_eval<IP, false, true, OBS>(bundle + oi, t, T.finv_hr, T.finv_hr2, unused,
+                                                drho_i, d2rho_i);
+            if (eam_j)
+                tabf_eval<IP, false, true, OBS>(bundle + oj, t, T.finv_hr, T.finv_hr2, unused,
+                                                drho_j, d2rho_j);
+        }
         float dedr = dV, X = 0.f, lap = 0.f;
         if (OBS) {
             X = d2V - dV * idr;
             lap = 2.f * (d2V + 2.f * dV * idr);
         }
         if (T.has_eam) {
-            // rho'_{t_i} and rho'_{t_j} at r: rho_a of the bundle belongs to the smaller type
-            int const oi = (ti <= tj) ? kFb : 2 * kFb, oj = (ti < tj) ? 2 * kFb : kFb;
-            float drho_i = 0.f, drho_j = 0.f, d2rho_i = 0.f, d2rho_j = 0.f, unused = 0.f;
-            if (!(dr > T.feam_rcut[ti]))
-                tabf_eval<IP, false, true, OBS>(bundle + oi, t, T.finv_hr, T.finv_hr2, unused,
-                                                drho_i, d2rho_i);
-            if (!(dr > T.feam_rcut[tj]))
-                tabf_eval<IP, false, true, OBS>(bundle + oj, t, T.finv_hr, T.finv_hr2, unused,
-                                                drho_j, d2rho_j);
             float const dFj = dFj2.x, dFi = in.dFi;
             // the two cross terms rounded separately and added commutatively: the pair
             // force is the same, bit for bit, seen from either atom
@@ -358,6 +426,12 @@ __device__ __forceinline__ void force_row_mx(AtomsView const &A, TablesView cons
                 lap += d2Fi * (drho_j * drho_j) + d2Fj * (drho_i * drho_i);
                 X += dFi * (d2rho_j - drho_j * idr) + dFj * (d2rho_i - drho_i * idr);
             }
+        }
+        if (!in_cut) {
+            dedr = 0.f;
+            V = 0.f;
+            X = 0.f;
+            lap = 0.f;
         }
         float const sc = __fmul_rn(-dedr, idr);
         fx += static_cast<double>(__fmul_rn(sc, dx));
@@ -406,18 +480,36 @@ __device__ __forceinline__ void force_row_mx(AtomsView const &A, TablesView cons
 // its lanes in FP64 first, which keeps the accumulators at 36 slots per group instead of
 // per thread (5.6 KB instead of 37 KB per block at 8 lanes per atom) and leaves that
 // shared memory to the L1 that caches the tables (measured 2-4 % faster).
-template <bool OBS, bool KICK, int TPA, int IP>
-__global__ void __launch_bounds__(kBlock) k_force_mx(AtomsView A, TablesView T) {
-    constexpr int kG = kBlock / TPA;
+//
+// STAGED: the block first copies the staged quintic tables (T.stf, T.st_bytes, about 180 KB
+// for a two-element alloy) into dynamic shared memory and reads every staged interval from
+// there, so table lookups no longer compete with the partner gathers for the L1 and never
+// miss to the L2. One such block fills an SM's shared memory, so it is NB = kBlockStaged
+// threads wide. Per-atom results equal the unstaged kernel's bit for bit; the global sums
+// differ only in the grouping of their FP64 partial sums.
+constexpr int kBlockStaged = kStagedBlock;
+
+template <bool OBS, bool KICK, int TPA, int IP, bool STAGED, typename IX,
+          int NB = STAGED ? kBlockStaged : kBlock>
+__global__ void __launch_bounds__(NB) k_force_mx(AtomsView A, TablesView T) {
+    constexpr int kG = NB / TPA;
     __shared__ double s_acc[F_NSUM * kG];
+    extern __shared__ float4 s_stage[];
     int const tid = threadIdx.x, grp = tid / TPA;
-    for (int k = tid; k < F_NSUM * kG; k += kBlock)
+    for (int k = tid; k < F_NSUM * kG; k += NB)
         s_acc[k] = 0.;
+    if (STAGED) {
+        const float4 *src = reinterpret_cast<const float4 *>(T.stf);
+        int const n16 = T.st_bytes / 16;
+        for (int k = tid; k < n16; k += NB)
+            s_stage[k] = __ldg(src + k);
+    }
     __syncthreads();
+    const float *stab = reinterpret_cast<const float *>(s_stage);
     int const r = A.fblk_rep[blockIdx.x];
     Replica const *R = A.rep + r;
     int const lb = blockIdx.x - R->fblk_begin, nb = R->fblk_n;
-    int const apb = kBlock / TPA, sub = tid % TPA;
+    int const apb = NB / TPA, sub = tid % TPA;
     int const n_slots = R->n_blocks * kBlock;
     RowIn in;
     box_f(R, in.L, in.iL);
@@ -438,13 +530,13 @@ __global__ void __launch_bounds__(kBlock) k_force_mx(AtomsView A, TablesView T) 
             in.dFi = dFi2.x;
             in.d2Fi = OBS ? dFi2.y : 0.f;
             int const nu = A.pn_up[i], nd = A.pn_dn[i];
-            int const *row = A.pnbr + static_cast<size_t>(i) * A.pmaxn;
+            PairRow<IX> const row = pair_row<IX>(A, i, R->atom_begin);
             bool warn_rmin = false;
             PairSums<OBS> ps;
-            force_row_mx<OBS, true, TPA, IP>(A, T, in, row, nu, sub, fx, fy, fz, epot, ps,
-                                             warn_rmin);
-            force_row_mx<OBS, false, TPA, IP>(A, T, in, row, nd, sub, fx, fy, fz, epot, ps,
-                                              warn_rmin);
+            force_row_mx<OBS, true, TPA, IP, STAGED, IX>(A, T, in, row, nu, sub, fx, fy, fz,
+                                                         epot, ps, warn_rmin, stab);
+            force_row_mx<OBS, false, TPA, IP, STAGED, IX>(A, T, in, row, nd, sub, fx, fy, fz,
+                                                          epot, ps, warn_rmin, stab);
             if (warn_rmin)
                 status_or(A.rep + r, MDELAST_WARN_RMIN);
             sums[F_VIRIAL] = (ps.sig_d[0] + ps.sig_d[1]) + ps.sig_d[2];
@@ -527,27 +619,82 @@ __global__ void __launch_bounds__(kBlock) k_force_mx(AtomsView A, TablesView T) 
     for (int k = 0; k < 15; ++k)
         acc[F_CB + k] *= kEv;
     acc[F_LAP] *= kEv / (kAng * kAng);
-    block_sum_store<F_NSUM>(acc, A.pf + static_cast<size_t>(blockIdx.x) * F_NSUM);
+    block_sum_store<F_NSUM, NB>(acc, A.pf + static_cast<size_t>(blockIdx.x) * F_NSUM);
 }
 
 namespace {
+template <bool OBS, int IP, typename IX>
+void density_mx_tpa_ix(int tpa, int grid, cudaStream_t s, AtomsView const &A,
+                       TablesView const &T) {
+    switch (tpa) {
+    case 1: k_density_mx<OBS, 1, IP, IX><<<grid, kBlock, 0, s>>>(A, T); break;
+    case 4: k_density_mx<OBS, 4, IP, IX><<<grid, kBlock, 0, s>>>(A, T); break;
+    case 8: k_density_mx<OBS, 8, IP, IX><<<grid, kBlock, 0, s>>>(A, T); break;
+    default: k_density_mx<OBS, 16, IP, IX><<<grid, kBlock, 0, s>>>(A, T); break;
+    }
+}
 template <bool OBS, int IP>
 void density_mx_tpa(int tpa, int grid, cudaStream_t s, AtomsView const &A, TablesView const &T) {
+    if (A.pnbr16)
+        density_mx_tpa_ix<OBS, IP, uint16_t>(tpa, grid, s, A, T);
+    else
+        density_mx_tpa_ix<OBS, IP, int>(tpa, grid, s, A, T);
+}
+template <bool OBS, bool KICK, int IP, typename IX>
+void force_mx_tpa_ix(int tpa, int grid, cudaStream_t s, AtomsView const &A,
+                     TablesView const &T) {
     switch (tpa) {
-    case 1: k_density_mx<OBS, 1, IP><<<grid, kBlock, 0, s>>>(A, T); break;
-    case 4: k_density_mx<OBS, 4, IP><<<grid, kBlock, 0, s>>>(A, T); break;
-    case 8: k_density_mx<OBS, 8, IP><<<grid, kBlock, 0, s>>>(A, T); break;
-    default: k_density_mx<OBS, 16, IP><<<grid, kBlock, 0, s>>>(A, T); break;
+    case 1: k_force_mx<OBS, KICK, 1, IP, false, IX><<<grid, kBlock, 0, s>>>(A, T); break;
+    case 4: k_force_mx<OBS, KICK, 4, IP, false, IX><<<grid, kBlock, 0, s>>>(A, T); break;
+    case 8: k_force_mx<OBS, KICK, 8, IP, false, IX><<<grid, kBlock, 0, s>>>(A, T); break;
+    default: k_force_mx<OBS, KICK, 16, IP, false, IX><<<grid, kBlock, 0, s>>>(A, T); break;
     }
 }
 template <bool OBS, bool KICK, int IP>
 void force_mx_tpa(int tpa, int grid, cudaStream_t s, AtomsView const &A, TablesView const &T) {
+    if (A.pnbr16)
+        force_mx_tpa_ix<OBS, KICK, IP, uint16_t>(tpa, grid, s, A, T);
+    else
+        force_mx_tpa_ix<OBS, KICK, IP, int>(tpa, grid, s, A, T);
+}
+// the staged kernels: lanes per atom 4, 8 or 16 (one lane per atom would need 143 KB of
+// accumulators beside the tables)
+template <bool OBS, bool KICK, typename IX>
+void force_mx_staged_ix(int tpa, int grid, cudaStream_t s, AtomsView const &A,
+                        TablesView const &T) {
+    size_t const smem = static_cast<size_t>(T.st_bytes);
+    constexpr int Q = MDELAST_QUINTIC;
     switch (tpa) {
-    case 1: k_force_mx<OBS, KICK, 1, IP><<<grid, kBlock, 0, s>>>(A, T); break;
-    case 4: k_force_mx<OBS, KICK, 4, IP><<<grid, kBlock, 0, s>>>(A, T); break;
-    case 8: k_force_mx<OBS, KICK, 8, IP><<<grid, kBlock, 0, s>>>(A, T); break;
-    default: k_force_mx<OBS, KICK, 16, IP><<<grid, kBlock, 0, s>>>(A, T); break;
+    case 4: k_force_mx<OBS, KICK, 4, Q, true, IX><<<grid, kBlockStaged, smem, s>>>(A, T); break;
+    case 8: k_force_mx<OBS, KICK, 8, Q, true, IX><<<grid, kBlockStaged, smem, s>>>(A, T); break;
+    default:
+        k_force_mx<OBS, KICK, 16, Q, true, IX><<<grid, kBlockStaged, smem, s>>>(A, T);
+        break;
     }
+}
+template <bool OBS, bool KICK>
+void force_mx_staged_tpa(int tpa, int grid, cudaStream_t s, AtomsView const &A,
+                         TablesView const &T) {
+    if (A.pnbr16)
+        force_mx_staged_ix<OBS, KICK, uint16_t>(tpa, grid, s, A, T);
+    else
+        force_mx_staged_ix<OBS, KICK, int>(tpa, grid, s, A, T);
+}
+template <bool OBS, bool KICK, typename IX> cudaError_t staged_attr_ix(int bytes) {
+    constexpr int Q = MDELAST_QUINTIC;
+    cudaFuncAttribute const a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    cudaError_t e = cudaFuncSetAttribute(k_force_mx<OBS, KICK, 4, Q, true, IX>, a, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_force_mx<OBS, KICK, 8, Q, true, IX>, a, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_force_mx<OBS, KICK, 16, Q, true, IX>, a, bytes);
+    return e;
+}
+template <bool OBS, bool KICK> cudaError_t staged_attr(int bytes) {
+    cudaError_t e = staged_attr_ix<OBS, KICK, int>(bytes);
+    if (e == cudaSuccess)
+        e = staged_attr_ix<OBS, KICK, uint16_t>(bytes);
+    return e;
 }
 template <int IP>
 void density_mx_ip(bool obs, int tpa, int grid, cudaStream_t s, AtomsView const &A,
@@ -585,6 +732,29 @@ void launch_force_mx(bool obs, bool kick, int tpa, int grid, cudaStream_t s, Ato
         force_mx_ip<MDELAST_BSPLINE>(obs, kick, tpa, grid, s, A, T);
     else
         force_mx_ip<MDELAST_QUINTIC>(obs, kick, tpa, grid, s, A, T);
+}
+
+void launch_force_mx_staged(bool obs, bool kick, int tpa, int grid, cudaStream_t s,
+                            AtomsView const &A, TablesView const &T) {
+    if (obs && kick)
+        force_mx_staged_tpa<true, true>(tpa, grid, s, A, T);
+    else if (obs)
+        force_mx_staged_tpa<true, false>(tpa, grid, s, A, T);
+    else if (kick)
+        force_mx_staged_tpa<false, true>(tpa, grid, s, A, T);
+    else
+        force_mx_staged_tpa<false, false>(tpa, grid, s, A, T);
+}
+
+cudaError_t prepare_force_mx_staged(int smem_bytes) {
+    cudaError_t e = staged_attr<true, true>(smem_bytes);
+    if (e == cudaSuccess)
+        e = staged_attr<true, false>(smem_bytes);
+    if (e == cudaSuccess)
+        e = staged_attr<false, true>(smem_bytes);
+    if (e == cudaSuccess)
+        e = staged_attr<false, false>(smem_bytes);
+    return e;
 }
 
 } // namespace mdelast

@@ -10,9 +10,10 @@ __device__ __forceinline__ void status_or(Replica *rep, unsigned bits) {
 }
 
 // Block-wide sum of NS per-thread values into out[0..NS), warp shuffles then shared
-// memory; deterministic for a fixed block size (kBlock threads).
-template <int NS> __device__ __forceinline__ void block_sum_store(double (&v)[NS], double *out) {
-    __shared__ double sm[kBlock / 32][NS];
+// memory; deterministic for a fixed block size (NB threads).
+template <int NS, int NB = kBlock>
+__device__ __forceinline__ void block_sum_store(double (&v)[NS], double *out) {
+    __shared__ double sm[NB / 32][NS];
     int const lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int k = 0; k < NS; ++k) {
@@ -27,7 +28,7 @@ template <int NS> __device__ __forceinline__ void block_sum_store(double (&v)[NS
     for (int k = threadIdx.x; k < NS; k += blockDim.x) {
         double s = 0.;
 #pragma unroll
-        for (int w = 0; w < kBlock / 32; ++w)
+        for (int w = 0; w < NB / 32; ++w)
             s += sm[w][k];
         out[k] = s;
     }
