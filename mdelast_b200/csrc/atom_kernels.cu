@@ -697,22 +697,35 @@ __global__ void __launch_bounds__(kBlock) k_kick_drift(AtomsView A, TablesView T
 
 // ------------------------------------------------------------------------------------
 // Pair list of the pair passes: the pairs of the neighbour list within sub_r2, the same
-// FP64 min-image test on both atoms of a pair (so the list is symmetric), in list order.
-// A replica's rows are rebuilt when its list was rebuilt or when some atom has moved by
-// more than half the radius margin since the last refresh: then every pair now within
-// r_cut is still in the list. One warp per atom slot at a time, grid-striding over the
-// slots; the warp takes 32 entries at a time and compacts the kept ones with a ballot. The
-// kernel runs every step and most steps refresh nothing: each block first asks whether any
-// replica is due (one flag per thread) and returns at once if none is, so a step without a
-// refresh costs one short wave instead of a warp per atom slot.
+// FP64 min-image test on both atoms of a pair (so the list is symmetric). A replica's rows
+// are rebuilt when its list was rebuilt or when some atom has moved by more than half the
+// radius margin since the last refresh: then every pair now within r_cut is still in the
+// list. One warp per atom slot at a time, grid-striding over the slots; the warp tests 32
+// entries at a time and compacts the kept ones with a ballot. The kernel runs every step
+// and most steps refresh nothing: each block first asks whether any replica is due (one
+// flag per thread) and returns at once if none is, so a step without a refresh costs one
+// short wave instead of a warp per atom slot.
+//
+// Row order (`sorted`, when the row fits the warp's shared-memory scratch): each half of a
+// row (partners j > i, partners j < i) is ordered by distance shell, shells kSubShell wide
+// in r/r_cut, in list order within a shell (a stable counting sort: the warp counts the
+// shells with shared-memory atomics, scans the counts, and places each chunk of 32 entries
+// with match_any). The lanes of a warp walk their rows in step, so at every iteration they
+// look up the tables at about the same r (the same neighbour shell of the lattice) and
+// read a few nearby intervals instead of scattered ones. Only the order in which an atom's
+// pair terms are summed changes; which pairs are kept does not.
+constexpr int kSubShells = 32;
+constexpr float kSubShell = 0.035f; // shell width / r_list; 32 shells reach 1.12 r_list
 
-__device__ __forceinline__ void sublist_row(AtomsView const &A, int i, int lane) {
+__device__ __forceinline__ void sublist_row(AtomsView const &A, int i, int lane, bool sorted,
+                                            int *s_j, int *s_cnt) {
     int const r = A.rep_of[i];
     if (r < 0)
         return;
     Replica const *R = A.rep + r;
     if (!(R->sub_force || R->sub_d2 > A.sub_half2))
         return;
+    sorted = sorted && R->n_atoms <= (1 << 26); // the packing holds 26-bit offsets
     double4 const ci = A.crd[i];
     double const hx = R->h[0], hy = R->h[1], hz = R->h[2];
     int const nu = A.n_up[i], nd = A.n_dn[i];
@@ -727,24 +740,82 @@ __device__ __forceinline__ void sublist_row(AtomsView const &A, int i, int lane)
             out[slot] = j;
     };
     unsigned const lt = (1u << lane) - 1u;
+    // shell of a squared distance: r / r_sub in units of kSubShell
+    float const inv_shell = 1.f / (kSubShell * static_cast<float>(sqrt(A.sub_r2)));
+    if (sorted) {
+        s_cnt[lane] = 0;
+        s_cnt[kSubShells + lane] = 0;
+        __syncwarp();
+    }
     int ku = 0, kd = 0;
     for (int k0 = 0; k0 < nu + nd; k0 += 32) {
         int const k = k0 + lane;
         bool keep = false, upper = k < nu;
         int j = -1;
+        double r2 = 0.;
         if (k < nu + nd) {
             j = row[upper ? k : A.maxn - 1 - (k - nu)];
             double px, py, pz;
-            keep = min_image_r2(ci, A.crd[j], hx, hy, hz, px, py, pz) <= A.sub_r2;
+            r2 = min_image_r2(ci, A.crd[j], hx, hy, hz, px, py, pz);
+            keep = r2 <= A.sub_r2;
         }
         unsigned const bu = __ballot_sync(0xffffffffu, keep && upper);
         unsigned const bd = __ballot_sync(0xffffffffu, keep && !upper);
-        if (keep && upper)
-            put(ku + __popc(bu & lt), j);
-        if (keep && !upper)
-            put(A.pmaxn - 1 - (kd + __popc(bd & lt)), j);
+        if (sorted) {
+            // kept entries to the scratch in list order (upper from the front, lower from
+            // the back) with their shell in the top bits; shells counted per half
+            if (keep) {
+                int const q = upper ? ku + __popc(bu & lt) : A.maxn - 1 - (kd + __popc(bd & lt));
+                int const sh = min(kSubShells - 1,
+                                   static_cast<int>(sqrtf(static_cast<float>(r2)) * inv_shell));
+                s_j[q] = (sh << 26) | (j - base);
+                atomicAdd(&s_cnt[(upper ? 0 : kSubShells) + sh], 1);
+            }
+        } else {
+            if (keep && upper)
+                put(ku + __popc(bu & lt), j);
+            if (keep && !upper)
+                put(A.pmaxn - 1 - (kd + __popc(bd & lt)), j);
+        }
         ku += __popc(bu);
         kd += __popc(bd);
+    }
+    if (sorted) {
+        __syncwarp();
+        for (int half = 0; half < 2; ++half) {
+            // exclusive scan of this half's shell counts: the shells' first output slots
+            int const c = s_cnt[half * kSubShells + lane];
+            int incl = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int const v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o)
+                    incl += v;
+            }
+            __syncwarp();
+            s_cnt[half * kSubShells + lane] = incl - c;
+            __syncwarp();
+            int const n_half = half ? kd : ku;
+            for (int e0 = 0; e0 < n_half; e0 += 32) {
+                int const e = e0 + lane;
+                bool const act = e < n_half;
+                int packed = 0, sh = kSubShells; // inactive lanes: a shell no entry has
+                if (act) {
+                    packed = s_j[half ? A.maxn - 1 - e : e];
+                    sh = packed >> 26;
+                }
+                unsigned const peers = __match_any_sync(0xffffffffu, sh);
+                if (act) {
+                    int const slot = s_cnt[half * kSubShells + sh] + __popc(peers & lt);
+                    put(half ? A.pmaxn - 1 - slot : slot, base + (packed & 0x3ffffff));
+                }
+                __syncwarp();
+                // the lowest lane of each shell's group advances that shell's next slot
+                if (act && (peers & lt) == 0)
+                    s_cnt[half * kSubShells + sh] += __popc(peers);
+                __syncwarp();
+            }
+        }
     }
     if (lane == 0) {
         A.pn_up[i] = ku;
@@ -753,7 +824,16 @@ __device__ __forceinline__ void sublist_row(AtomsView const &A, int i, int lane)
     }
 }
 
+// dynamic shared memory of k_sublist: per warp of its 256-thread blocks, one row of packed
+// entries (maxn) and two halves' shell counters; 0 when that exceeds kSublistSortMax or a
+// replica offset does not fit the packing (the rows then keep list order)
+__host__ __device__ size_t sublist_smem(int maxn) {
+    size_t const b = static_cast<size_t>(256 / 32) * (maxn + 2 * kSubShells) * sizeof(int);
+    return b <= kSublistSortMax ? b : 0;
+}
+
 __global__ void __launch_bounds__(256) k_sublist(AtomsView A) {
+    extern __shared__ int s_sub[];
     int due = 0;
     for (int r = threadIdx.x; r < A.n_rep; r += blockDim.x) {
         Replica const *R = A.rep + r;
@@ -761,10 +841,13 @@ __global__ void __launch_bounds__(256) k_sublist(AtomsView A) {
     }
     if (!__syncthreads_or(due))
         return;
-    int const lane = threadIdx.x & 31;
+    int const lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    bool const sorted = sublist_smem(A.maxn) > 0;
+    int *s_j = s_sub + static_cast<size_t>(warp) * (A.maxn + 2 * kSubShells);
+    int *s_cnt = s_j + A.maxn;
     int const n_warps = gridDim.x * (blockDim.x >> 5);
     for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < A.n_pad; i += n_warps)
-        sublist_row(A, i, lane);
+        sublist_row(A, i, lane, sorted, s_j, s_cnt);
 }
 
 __global__ void k_sub_invalidate(AtomsView A) {

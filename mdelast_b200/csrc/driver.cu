@@ -218,8 +218,13 @@ struct mdelast_driver_s {
     int set_pair_list(double factor);
     void point_pair_list();
     void refresh_pair_list(cudaStream_t s) {
-        if (A.crd_ref)
-            k_sublist<<<std::min(n_pad / 8, kSublistBlocks), 256, 0, s>>>(A);
+        if (A.crd_ref) {
+            size_t const smem = sublist_smem(A.maxn);
+            if (smem > 48 * 1024)
+                cudaFuncSetAttribute(k_sublist, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(smem));
+            k_sublist<<<std::min(n_pad / 8, kSublistBlocks), 256, smem, s>>>(A);
+        }
     }
     double *d_pd = nullptr, *d_pf = nullptr, *d_red = nullptr;
     size_t cap_dmap = 0, cap_fmap = 0, cap_pd = 0, cap_pf = 0, cap_red = 0; // elements

@@ -39,6 +39,9 @@ __global__ void k_reduce(AtomsView A);
 __global__ void k_post(AtomsView A, int mode, int obs);
 __global__ void k_samples_reset(AtomsView A, int what);
 __global__ void k_sublist(AtomsView A);
+// k_sublist's dynamic shared memory for rows of capacity maxn (0: rows keep list order)
+constexpr size_t kSublistSortMax = 96 * 1024;
+__host__ __device__ size_t sublist_smem(int maxn);
 __global__ void k_sub_invalidate(AtomsView A);
 __global__ void k_readout(AtomsView A, TablesView T, int r, int field, double *out,
                           const double *pos0, int stepped);
