@@ -169,25 +169,28 @@ __global__ void __launch_bounds__(kBlock) k_density_mx(AtomsView A, TablesView T
             int const nu = A.pn_up[i], ntot = nu + A.pn_dn[i];
             PairRow<IX> const row = pair_row<IX>(A, i, R->atom_begin);
             float4 pn = A.posf[sub < ntot ? row.at(list_slot(sub, nu, A.pmaxn)) : i];
+            // branch-free body, two entries per unrolled pass, as in the force pass: an
+            // entry beyond the cutoff adds zeros
+#pragma unroll 2
             for (int kk = sub; kk < ntot; kk += TPA) {
                 float4 const pj = pn;
-                if (kk + TPA < ntot)
-                    pn = A.posf[row.at(list_slot(kk + TPA, nu, A.pmaxn))];
+                pn = A.posf[row.at(list_slot(min(kk + TPA, ntot - 1), nu, A.pmaxn))];
                 float dx, dy, dz;
                 float const r2 = min_image_f(pi, pj, L, iL, dx, dy, dz);
-                if (r2 > T.fr_cut_sq)
-                    continue;
                 float const idr = rsqrtf(r2);
                 float const dr = __fmul_rn(r2, idr);
                 int const tj = static_cast<int>(pj.w);
-                if (dr > T.feam_rcut[tj])
-                    continue;
+                bool const in_cut = !(r2 > T.fr_cut_sq) && !(dr > T.feam_rcut[tj]);
                 float t;
                 int const k = tab_locate_f(dr, T.finv_hr, T.nri, t);
                 float v = 0.f, d1 = 0.f, d2 = 0.f;
                 tabf_eval<IP, true, OBS, false>(
                     T.rrf + (static_cast<size_t>(tj) * T.nri + k) * TabFmt<IP>::kFf, t,
                     T.finv_hr, T.finv_hr2, v, d1, d2);
+                if (!in_cut) {
+                    v = 0.f;
+                    d1 = 0.f;
+                }
                 rho += static_cast<double>(v);
                 if (OBS) {
                     float const ar = d1 * idr;
