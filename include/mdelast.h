@@ -302,6 +302,14 @@ int mdelast_driver_set_launch(mdelast_driver *d, int32_t tpa_density, int32_t tp
  * and block target; MDELAST_ERR_UNSUPPORTED when no staged copy exists. get: *on the
  * variant in use, *available whether a staged copy exists (either may be NULL). */
 int mdelast_driver_set_force_staging(mdelast_driver *d, int32_t on);
+/* Neighbour-list capacity per atom (*maxn) and how many step launches were resumed after
+ * an in-step list rebuild outgrew it (*regrowths); either may be NULL. The reference grows
+ * its list whenever it needs to (md_driver.cpp:288-292); here an in-step rebuild that
+ * overflows stops the launch's remaining steps on the device (their kernels return without
+ * work), and the next wait for results grows the capacity and runs those steps again, so
+ * run()/integrate_n() continue instead of failing. MDELAST_LIST_HEADROOM (default 0.5)
+ * sets the headroom h of a new capacity: (1 + h) x the largest count, + 32 when h > 0. */
+int mdelast_driver_list_capacity(mdelast_driver *d, int32_t *maxn, int32_t *regrowths);
 int mdelast_driver_get_force_staging(mdelast_driver *d, int32_t *on, int32_t *available);
 /* The list the pair passes walk. No counterpart in the reference (its passes walk the
  * neighbour list, whose pairs beyond r_cut they skip). factor > 1: the neighbour list's

@@ -61,8 +61,10 @@ __global__ void k_cell_bin(AtomsView A) {
     int const pos = atomicAdd(&A.cell_count[cell], 1);
     if (pos < A.cell_cap)
         A.cell_atoms[static_cast<size_t>(cell) * A.cell_cap + pos] = i;
-    else
+    else {
         status_or(&A.rep[r], MDELAST_ERR_CELL_OVERFLOW);
+        set_halt(A);
+    }
 }
 
 // Order each cell's members by slot index (rank sort in shared memory), so that the list
@@ -264,8 +266,10 @@ __global__ void __launch_bounds__(128) k_nbr_cells(AtomsView A) {
         int const i = me[a];
         A.n_up[i] = c_nu[a];
         A.n_dn[i] = c_nd[a];
-        if (c_tot[a] > A.maxn)
+        if (c_tot[a] > A.maxn) {
             status_or(&A.rep[r], MDELAST_ERR_LIST_OVERFLOW);
+            set_halt(A);
+        }
         atomicMax(&A.max_count[0], c_tot[a]);
     }
 }
@@ -346,8 +350,10 @@ __global__ void k_nbr_build(AtomsView A, int cells_done) {
     if (lane == 0) {
         A.n_up[i] = nu;
         A.n_dn[i] = nd;
-        if (total > A.maxn)
+        if (total > A.maxn) {
             status_or(&A.rep[r], MDELAST_ERR_LIST_OVERFLOW);
+            set_halt(A);
+        }
         atomicMax(&A.max_count[0], total);
     }
 }
@@ -361,6 +367,8 @@ __global__ void k_nbr_build(AtomsView A, int cells_done) {
 
 template <bool OBS, int TPA, int IP, typename IX>
 __global__ void __launch_bounds__(kBlock) k_density(AtomsView A, TablesView T) {
+    if (halted(A)) // a list build ran out of capacity: nothing until the host regrows
+        return;
     constexpr int kF = TabFmt<IP>::kF;
     int const r = A.dblk_rep[blockIdx.x];
     Replica const *R = A.rep + r;
@@ -472,6 +480,8 @@ __global__ void __launch_bounds__(kBlock) k_density(AtomsView A, TablesView T) {
 
 template <bool OBS, bool KICK, int TPA, int IP, typename IX>
 __global__ void __launch_bounds__(kBlock) k_force(AtomsView A, TablesView T) {
+    if (halted(A)) // a list build ran out of capacity: nothing until the host regrows
+        return;
     constexpr int kF = TabFmt<IP>::kF;
     int const r = A.fblk_rep[blockIdx.x];
     Replica const *R = A.rep + r;
@@ -645,6 +655,8 @@ __global__ void __launch_bounds__(kBlock) k_force(AtomsView A, TablesView T) {
 // c += (cf dt) v / h with the box before this step's barostat update.
 
 __global__ void __launch_bounds__(kBlock) k_kick_drift(AtomsView A, TablesView T) {
+    if (halted(A)) // a list build ran out of capacity: nothing until the host regrows
+        return;
     // the grid covers the n_pad slots exactly; a warp never spans two replicas (their
     // ranges start on multiples of kTile) and its padding slots, if any, come last
     int const i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -833,6 +845,8 @@ __host__ __device__ size_t sublist_smem(int maxn) {
 }
 
 __global__ void __launch_bounds__(256) k_sublist(AtomsView A) {
+    if (halted(A)) // a list build ran out of capacity: nothing until the host regrows
+        return;
     extern __shared__ int s_sub[];
     int due = 0;
     for (int r = threadIdx.x; r < A.n_rep; r += blockDim.x) {

@@ -155,6 +155,11 @@ struct AtomsView {
     int *pnbr, *pn_up, *pn_dn;
     uint16_t *pnbr16;
     int pmaxn, pad_p;
+    // Set (to 1) by a list build that ran out of neighbour or cell capacity. Every kernel
+    // of a step returns at once while it is set, so the steps of a launch after an
+    // overflowing in-step rebuild change nothing; the host grows the capacity and resumes
+    // from the last completed step.
+    int *halt;
     double4 *crd_ref;     // null: the pair passes read the neighbour list
     double sub_r2, sub_half2;
 };

@@ -234,6 +234,15 @@ struct mdelast_driver_s {
         k_post<<<n_rep, 256, 0, s>>>(A, mode, obs);
     }
     int *d_cell_count = nullptr, *d_cell_atoms = nullptr, *d_max_count = nullptr;
+    int *d_halt = nullptr; // AtomsView::halt
+    // The last launch of steps, for resuming it after a list build ran out of capacity in
+    // one of its steps: cycle before it, steps, rebuild and sampling cadence.
+    struct Launch {
+        bool resumable = false;
+        unsigned long long start = 0;
+        int n = 0, rebuild_every = 0, sample_every = 0;
+    } last_launch;
+    int resume_after_overflow();
     int *d_cell_rep = nullptr;
     std::vector<int> cell_rep_host; // replica of each cell, as uploaded
     double *d_rb = nullptr, *d_Ft = nullptr;
@@ -260,6 +269,7 @@ struct mdelast_driver_s {
     cudaEvent_t ev_step = nullptr;
     cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr}; // [2 * rebuild + obs]
     unsigned long long host_cycle = 0; // steps launched (the reference's cycle counter)
+    int list_regrowths = 0;            // launches resumed after a list overflow
     bool all_pairs = false; // every replica lists by all-pairs search
 
     ~mdelast_driver_s();
@@ -323,6 +333,7 @@ mdelast_driver_s::~mdelast_driver_s() {
     dfree(d_cell_atoms);
     dfree(d_cell_rep);
     dfree(d_max_count);
+    dfree(d_halt);
     dfree(d_rb);
     dfree(d_Ft);
     dfree(d_pos0);
@@ -659,6 +670,17 @@ int mdelast_driver_s::enqueue_rebuild() {
     return MDELAST_OK;
 }
 
+// Headroom of neighbour-list capacities: a new capacity is (1 + h) times the largest count
+// plus 32 (plus nothing when h is 0); MDELAST_LIST_HEADROOM sets h (default 0.5).
+double list_headroom() {
+    if (char const *e = std::getenv("MDELAST_LIST_HEADROOM")) {
+        double const h = std::atof(e);
+        if (h >= 0. && h <= 16.)
+            return h;
+    }
+    return 0.5;
+}
+
 // Build the list now and grow the neighbour or cell capacity until it fits.
 int mdelast_driver_s::build_list_checked() {
     for (int attempt = 0; attempt < 6; ++attempt) {
@@ -674,13 +696,16 @@ int mdelast_driver_s::build_list_checked() {
             grow = true;
         }
         if (mc[0] > A.maxn) {
-            int const m = ((mc[0] + mc[0] / 2 + 32) + 3) / 4 * 4;
-            if (int rc = alloc_list(m))
+            double const h = list_headroom();
+            int const m = (static_cast<int>(mc[0] * (1. + h)) + (h > 0. ? 32 : 0) + 3) / 4 * 4;
+            if (int rc = alloc_list(std::max(m, mc[0])))
                 return rc;
             grow = true;
         }
-        if (!grow)
+        if (!grow) {
+            CK(cudaMemsetAsync(d_halt, 0, sizeof(int), stream));
             return MDELAST_OK;
+        }
         // the overflow bits of the attempt that did not fit
         k_status_and<<<1, 32, 0, stream>>>(A, ~(MDELAST_ERR_LIST_OVERFLOW | MDELAST_ERR_CELL_OVERFLOW));
         CK(cudaGetLastError());
@@ -732,6 +757,11 @@ int mdelast_driver_s::step_graph(int obs, int rebuild, cudaGraphExec_t *out) {
 
 // Launch n steps; rebuild_every / sample_every < 0 mean "never" / "use the flag".
 int mdelast_driver_s::launch_steps(int n_steps, int rebuild_every, int sample_every) {
+    last_launch.resumable = neighbors && rebuild_every > 0;
+    last_launch.start = host_cycle;
+    last_launch.n = n_steps;
+    last_launch.rebuild_every = rebuild_every;
+    last_launch.sample_every = sample_every;
     for (int s = 0; s < n_steps; ++s) {
         unsigned long long const c = host_cycle;
         int const rebuild = rebuild_every > 0 && c % static_cast<unsigned>(rebuild_every) == 0;
@@ -760,9 +790,47 @@ int mdelast_driver_s::wait_step() {
     return check_status();
 }
 
+// An in-step list rebuild ran out of neighbour or cell capacity (as the reference's list
+// grows, md_driver.cpp:288-292): the kernels of that step and of every later step of the
+// launch returned without work. Grow the capacity, rebuild at the unchanged positions and
+// launch the remaining steps again, until the launch completes.
+int mdelast_driver_s::resume_after_overflow() {
+    unsigned const bits = MDELAST_ERR_LIST_OVERFLOW | MDELAST_ERR_CELL_OVERFLOW;
+    for (int attempt = 0; attempt < 64; ++attempt) {
+        bool over = false;
+        for (int r = 0; r < n_rep; ++r)
+            over = over || (h_obs[r].status & bits) != 0;
+        if (!over)
+            return MDELAST_OK;
+        if (!last_launch.resumable)
+            return MDELAST_OK; // reported as fatal by check_status
+        // every replica completed the same steps: their cycle counters agree
+        unsigned long long const done = static_cast<unsigned long long>(h_obs[0].cycle);
+        if (done < last_launch.start || done > last_launch.start + last_launch.n)
+            return fail(MDELAST_ERR_CUDA, "inconsistent cycle after a list overflow");
+        int const left = static_cast<int>(last_launch.start + last_launch.n - done);
+        k_status_and<<<1, 32, 0, stream>>>(A, ~bits);
+        CK(cudaGetLastError());
+        for (int r = 0; r < n_rep; ++r)
+            h_obs[r].status &= ~bits;
+        host_cycle = done;
+        if (int rc = configure_cells(current_boxes()))
+            return rc;
+        if (int rc = build_list_checked()) // grows, rebuilds and clears the halt
+            return rc;
+        if (int rc = launch_steps(left, last_launch.rebuild_every, last_launch.sample_every))
+            return rc;
+        CK(cudaEventSynchronize(ev_step));
+        ++list_regrowths;
+    }
+    return fail(MDELAST_ERR_CAPACITY, "neighbour list kept overflowing after repeated growth");
+}
+
 int mdelast_driver_s::check_status() {
     if (dead)
         return fail(MDELAST_ERR_FATAL, "%s (status 0x%x)", fatal_message(dead_bits), dead_bits);
+    if (int rc = resume_after_overflow())
+        return rc;
     for (int r = 0; r < n_rep; ++r) {
         unsigned const st = h_obs[r].status;
         if (st & MDELAST_FATAL_MASK) {
@@ -1222,6 +1290,7 @@ static int create_system(const mdelast_driver_config *cfgs, int n_rep, mdelast_d
     TRY(dalloc(&d->d_red, static_cast<size_t>(n_rep) * max_chunks * 64));
     d->cap_red = static_cast<size_t>(n_rep) * max_chunks * 64;
     TRY(dalloc(&d->d_max_count, 2));
+    TRY(dalloc(&d->d_halt, 1));
     TRY(dalloc(&d->d_pos0, pos0.size()));
     int max_n = 0;
     for (int r = 0; r < n_rep; ++r)
@@ -1262,6 +1331,7 @@ static int create_system(const mdelast_driver_config *cfgs, int n_rep, mdelast_d
     A.dblk_rep = d->d_dblk_rep;
     A.fblk_rep = d->d_fblk_rep;
     A.max_count = d->d_max_count;
+    A.halt = d->d_halt;
     TRY(d->alloc_ring(MDELAST_DEFAULT_SAMPLE_RING));
     if (d->neighbors) // md_driver.cpp:42: pow<2>(pot[0]->rcut * r_skin)
         A.r_list_sq = (rcut * c0.r_skin) * (rcut * c0.r_skin);
@@ -1274,7 +1344,9 @@ static int create_system(const mdelast_driver_config *cfgs, int n_rep, mdelast_d
         mdelast_driver_config const &c = cfgs[r];
         double const vol = c.box[0] * (c.box[4] * c.box[8]);
         double const mean = 4. / 3. * M_PI * std::pow(d->r_list, 3) * c.n_atoms / vol;
-        int m = static_cast<int>(1.5 * std::min(mean, static_cast<double>(c.n_atoms))) + 32;
+        double const h = list_headroom();
+        int m = static_cast<int>((1. + h) * std::min(mean, static_cast<double>(c.n_atoms))) +
+                (h > 0. ? 32 : 0);
         m = std::min((m + 3) / 4 * 4, (c.n_atoms + 3) / 4 * 4);
         maxn = std::max(maxn, m);
     }
@@ -1758,6 +1830,17 @@ int mdelast_driver_set_launch(mdelast_driver *d, int32_t tpa_density, int32_t tp
         return rc;
     double md = 0., mf = 0.;
     return d->time_passes(1, 1, &md, &mf);
+}
+
+int mdelast_driver_list_capacity(mdelast_driver *d, int32_t *maxn, int32_t *regrowths) {
+    clear_error();
+    if (!d)
+        return fail(MDELAST_ERR_ARGUMENT, "null driver");
+    if (maxn)
+        *maxn = d->A.maxn;
+    if (regrowths)
+        *regrowths = d->list_regrowths;
+    return MDELAST_OK;
 }
 
 int mdelast_driver_set_force_staging(mdelast_driver *d, int32_t on) {

@@ -559,6 +559,11 @@ class MDDriver {
     void set_sample_ring(int capacity) { check(mdelast_driver_set_sample_ring(d_, capacity)); }
     py::dict autotune(int n_repeat) { return autotune_dict(d_, n_repeat); }
     py::object force_staging() { return force_staging_get(d_); }
+    py::tuple list_capacity() {
+        int32_t m = 0, g = 0;
+        check(mdelast_driver_list_capacity(d_, &m, &g));
+        return py::make_tuple(m, g);
+    }
     void set_force_staging(bool on) { check(mdelast_driver_set_force_staging(d_, on ? 1 : 0)); }
     void set_launch(int td, int tf, int bd, int bf) {
         check(mdelast_driver_set_launch(d_, td, tf, bd, bf));
@@ -853,6 +858,11 @@ class BatchedMDDriver {
     void set_sample_ring(int capacity) { check(mdelast_driver_set_sample_ring(d_, capacity)); }
     py::dict autotune(int n_repeat) { return autotune_dict(d_, n_repeat); }
     py::object force_staging() { return force_staging_get(d_); }
+    py::tuple list_capacity() {
+        int32_t m = 0, g = 0;
+        check(mdelast_driver_list_capacity(d_, &m, &g));
+        return py::make_tuple(m, g);
+    }
     void set_force_staging(bool on) { check(mdelast_driver_set_force_staging(d_, on ? 1 : 0)); }
     void set_launch(int td, int tf, int bd, int bf) {
         check(mdelast_driver_set_launch(d_, td, tf, bd, bf));
@@ -1042,6 +1052,8 @@ PYBIND11_MODULE(md_driver_module, m) {
              py::arg("blocks_density"), py::arg("blocks_force"))
         .def_property("force_staging", &MDDriver::force_staging, &MDDriver::set_force_staging,
                       "force pass reading shared-memory tables (None: no staged copy)")
+        .def_property_readonly("list_capacity", &MDDriver::list_capacity,
+                               "(neighbour slots per atom, launches resumed after a list overflow)")
         .def("set_pair_list", &MDDriver::set_pair_list, py::arg("factor"),
              "pair passes walk the list's pairs within factor * r_cut (0: the full list)")
         .def("set_sample_ring", &MDDriver::set_sample_ring, py::arg("capacity"),
@@ -1105,6 +1117,7 @@ PYBIND11_MODULE(md_driver_module, m) {
              py::arg("tpa_force"), py::arg("blocks_density"), py::arg("blocks_force"))
         .def_property("force_staging", &BatchedMDDriver::force_staging,
                       &BatchedMDDriver::set_force_staging)
+        .def_property_readonly("list_capacity", &BatchedMDDriver::list_capacity)
         .def("set_pair_list", &BatchedMDDriver::set_pair_list, py::arg("factor"))
         .def("set_sample_ring", &BatchedMDDriver::set_sample_ring, py::arg("capacity"))
         .def("drain_samples", &BatchedMDDriver::drain_samples, py::arg("replica"))

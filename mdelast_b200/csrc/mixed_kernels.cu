@@ -142,6 +142,8 @@ __device__ __forceinline__ void warp_accumulate(double v, double *slot) {
 // partner gathers.
 template <bool OBS, int TPA, int IP, typename IX>
 __global__ void __launch_bounds__(kBlock) k_density_mx(AtomsView A, TablesView T) {
+    if (halted(A)) // a list build ran out of capacity: nothing until the host regrows
+        return;
     constexpr int kF = TabFmt<IP>::kF;
     __shared__ double sacc[kBlock / 32][D_NSUM];
     int const warp = threadIdx.x >> 5;
@@ -495,6 +497,8 @@ constexpr int kBlockStaged = kStagedBlock;
 template <bool OBS, bool KICK, int TPA, int IP, bool STAGED, typename IX,
           int NB = STAGED ? kBlockStaged : kBlock>
 __global__ void __launch_bounds__(NB) k_force_mx(AtomsView A, TablesView T) {
+    if (halted(A)) // a list build ran out of capacity: nothing until the host regrows
+        return;
     constexpr int kG = NB / TPA;
     __shared__ double s_acc[F_NSUM * kG];
     extern __shared__ float4 s_stage[];

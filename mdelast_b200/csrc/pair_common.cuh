@@ -9,6 +9,10 @@ __device__ __forceinline__ void status_or(Replica *rep, unsigned bits) {
     atomicOr(&rep->obs.status, bits);
 }
 
+// a list build ran out of capacity: the rest of the launch's steps are skipped
+__device__ __forceinline__ bool halted(AtomsView const &A) { return *A.halt != 0; }
+__device__ __forceinline__ void set_halt(AtomsView const &A) { *A.halt = 1; }
+
 // Block-wide sum of NS per-thread values into out[0..NS), warp shuffles then shared
 // memory; deterministic for a fixed block size (NB threads).
 template <int NS, int NB = kBlock>

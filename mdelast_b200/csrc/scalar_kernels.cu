@@ -356,6 +356,8 @@ __device__ __forceinline__ void replica_store(Replica const *s, Replica *g) {
 // half steps, U2p, and the coefficients of the opening kick and of the drift, with the
 // NPT box update of U1 (md_driver.cpp:488-498).
 __global__ void k_pre(AtomsView A) {
+    if (*A.halt) // a list build ran out of capacity: nothing until the host regrows
+        return;
     Replica *R = A.rep + blockIdx.x;
     __shared__ double s_S, s_ekin;
     int const ens = R->ensemble;
@@ -417,6 +419,8 @@ __global__ void k_pre(AtomsView A) {
 // (c, r) adds blocks [c kChunk, (c+1) kChunk) of replica r for every slot, in a fixed
 // order, spreading the reduction over many SMs (k_post then adds the chunk sums).
 __global__ void k_reduce(AtomsView A) {
+    if (*A.halt) // a list build ran out of capacity: nothing until the host regrows
+        return;
     Replica const *R = A.rep + blockIdx.y;
     int const c = blockIdx.x;
     int const g = threadIdx.x >> 6, q = threadIdx.x & 63;
@@ -555,6 +559,8 @@ __device__ void thermodynamics(Replica *R, int mode, int obs, const double *sf, 
                                double S, double ekin, double virial);
 
 __global__ void k_post(AtomsView A, int mode, int obs) {
+    if (*A.halt) // a list build ran out of capacity: nothing until the host regrows
+        return;
     __shared__ Replica sR;
     __shared__ double sf[F_NSUM], sd[D_NSUM];
     __shared__ double s_part[4][F_NSUM + D_NSUM];
