@@ -198,9 +198,10 @@ int mdelast_driver_calculate_neighbors(mdelast_driver *d);
  * step that starts at cycle c the list is rebuilt when rebuild_every > 0 and
  * c % rebuild_every == 0 (drivers with neighbors=1), and the step samples the Born tensor
  * and Laplacian when sample_every > 0 and (c + 1) % sample_every == 0. The rebuilds run on
- * the device inside the step graph with the current capacities (an overflow is reported
- * like a FATAL). If device_ms is not NULL the call waits for the steps and stores their
- * duration measured with CUDA events on the driver's stream. */
+ * the device inside the step graph; one that outgrows the neighbour capacity stops the
+ * remaining steps, and the next wait for results grows the capacity and runs them
+ * (mdelast_driver_list_capacity). If device_ms is not NULL the call waits for the steps and
+ * stores their duration measured with CUDA events on the driver's stream. */
 int mdelast_driver_run(mdelast_driver *d, int32_t n_steps, int32_t rebuild_every,
                        int32_t sample_every, float *device_ms);
 /* Diagnostics: run n_steps sampled steps with a CUDA event between consecutive kernels
@@ -292,6 +293,15 @@ int mdelast_driver_autotune(mdelast_driver *d, int32_t n_repeat, int32_t *choice
                             double *ms_out);
 int mdelast_driver_set_launch(mdelast_driver *d, int32_t tpa_density, int32_t tpa_force,
                               int32_t blocks_density, int32_t blocks_force);
+/* The same choice made on real steps: each candidate shape runs n_steps sampled steps of
+ * run(n, rebuild_every, 1) (the state advances: use it as part of a warm-up), and the
+ * passes are timed in the cache state a step leaves them, which repeated passes on a fixed
+ * state (autotune) do not reproduce. The density pass is tuned first over lanes per atom
+ * {1, 4, 8, 16} x {16, 32, 64} x 148 blocks, then the force pass over {1, 4, 8, 16} x
+ * {8, 16, 32} x 148 and, where tables are staged, the staged pass at {4, 8} x {4, 8} x 148.
+ * About 30 n_steps steps in all. choice and ms_out as for autotune. */
+int mdelast_driver_autotune_steps(mdelast_driver *d, int32_t n_steps, int32_t rebuild_every,
+                                  int32_t *choice, double *ms_out);
 /* The staged force pass. No counterpart in the reference. In mixed precision with quintic
  * EAM tables, a driver keeps an FP32 copy of the top intervals of every phi_ab and rho_a
  * (those up to the largest cutoff, at most 184 KB; each function once), and the staged

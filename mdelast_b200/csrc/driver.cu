@@ -283,7 +283,9 @@ struct mdelast_driver_s {
     std::vector<long> pos0_off;            // offset of each replica in d_pos0
     int enqueue_rebuild();
     int build_list_checked();
-    int enqueue_step(int obs, int rebuild);
+    int enqueue_step(int obs, int rebuild, cudaEvent_t const *ev = nullptr);
+    int time_steps(int n, int rebuild_every, double *ms_d, double *ms_f);
+    int tune_on_steps(int n, int rebuild_every, int *choice, double *ms);
     int step_graph(int obs, int rebuild, cudaGraphExec_t *out);
     int launch_steps(int n_steps, int rebuild_every, int sample_every);
     int wait_step();
@@ -522,6 +524,109 @@ int mdelast_driver_s::set_launch(int tpa_d_, int tpa_f_, int tgt_d, int tgt_f, i
     return MDELAST_OK;
 }
 
+// n real steps, launched one by one with events around the two pair passes (the state
+// advances exactly as in run(n, rebuild_every, 1)); mean device time of the density and
+// the force pass over them. The passes then run in the cache state a step leaves them,
+// which repeated passes on a fixed state do not reproduce.
+int mdelast_driver_s::time_steps(int n, int rebuild_every, double *ms_d, double *ms_f) {
+    cudaEvent_t ev[3];
+    for (auto &e : ev)
+        CK(cudaEventCreate(&e));
+    double td = 0., tf = 0.;
+    int rc = MDELAST_OK;
+    for (int k = 0; k < n && !rc; ++k) {
+        unsigned long long const c = host_cycle;
+        int const rebuild = neighbors && rebuild_every > 0 &&
+                            c % static_cast<unsigned>(rebuild_every) == 0;
+        // a one-step launch, resumable like run()'s after a list overflow
+        last_launch.resumable = neighbors && rebuild_every > 0;
+        last_launch.start = c;
+        last_launch.n = 1;
+        last_launch.rebuild_every = rebuild_every;
+        last_launch.sample_every = 1;
+        rc = enqueue_step(1, rebuild, ev);
+        if (rc)
+            break;
+        ++host_cycle;
+        cudaError_t const e = cudaEventRecord(ev_step, stream);
+        if (e != cudaSuccess) {
+            rc = fail(MDELAST_ERR_CUDA, "step timing: %s", cudaGetErrorString(e));
+            break;
+        }
+        obs_valid = false;
+        stepped = true;
+        rc = wait_step();
+        if (rc)
+            break;
+        float a = 0.f, b = 0.f;
+        cudaEventElapsedTime(&a, ev[0], ev[1]);
+        cudaEventElapsedTime(&b, ev[1], ev[2]);
+        td += a;
+        tf += b;
+    }
+    for (auto &e : ev)
+        cudaEventDestroy(e);
+    if (rc)
+        return rc;
+    *ms_d = td / n;
+    *ms_f = tf / n;
+    return MDELAST_OK;
+}
+
+// The launch shapes timed on real steps (time_steps): first the density pass over its
+// shapes with the force shape fixed, then the force pass (both variants) with the best
+// density shape; n steps per shape.
+int mdelast_driver_s::tune_on_steps(int n, int rebuild_every, int *choice, double *ms) {
+    double best_d = 1e300, best_f = 1e300;
+    int bd[2] = {tpa_d, target_d}, bf[3] = {tpa_f, target_f, stage_f ? 1 : 0};
+    for (int tp : {1, 4, 8, 16})
+        for (int tg : {148 * 16, 148 * 32, 148 * 64}) {
+            if (int rc = set_launch(tp, bf[0], tg, bf[1], bf[2]))
+                return rc;
+            double md = 0., mf = 0.;
+            if (int rc = time_steps(n, rebuild_every, &md, &mf))
+                return rc;
+            if (md < best_d) {
+                best_d = md;
+                bd[0] = tp;
+                bd[1] = tg;
+            }
+        }
+    struct Shape {
+        int tpa, target, staged;
+    };
+    std::vector<Shape> shapes;
+    for (int tp : {1, 4, 8, 16})
+        for (int tg : {148 * 8, 148 * 16, 148 * 32})
+            shapes.push_back({tp, tg, 0});
+    if (staging_available())
+        for (int tp : {4, 8})
+            for (int tg : {148 * 4, 148 * 8})
+                shapes.push_back({tp, tg, 1});
+    for (Shape const &x : shapes) {
+        if (int rc = set_launch(bd[0], x.tpa, bd[1], x.target, x.staged))
+            return rc;
+        double md = 0., mf = 0.;
+        if (int rc = time_steps(n, rebuild_every, &md, &mf))
+            return rc;
+        if (mf < best_f) {
+            best_f = mf;
+            bf[0] = x.tpa;
+            bf[1] = x.target;
+            bf[2] = x.staged;
+        }
+    }
+    if (int rc = set_launch(bd[0], bf[0], bd[1], bf[1], bf[2]))
+        return rc;
+    choice[0] = bd[0];
+    choice[1] = bf[0];
+    choice[2] = bd[1];
+    choice[3] = bf[1];
+    ms[0] = best_d;
+    ms[1] = best_f;
+    return MDELAST_OK;
+}
+
 // Mean device time of the density and the force pass (no kick: the state is unchanged)
 // over n_repeat launches on the current positions, after one untimed pair.
 int mdelast_driver_s::time_passes(int n_repeat, int obs, double *ms_d, double *ms_f) {
@@ -713,7 +818,7 @@ int mdelast_driver_s::build_list_checked() {
     return fail(MDELAST_ERR_CAPACITY, "neighbour list did not fit after repeated growth");
 }
 
-int mdelast_driver_s::enqueue_step(int obs, int rebuild) {
+int mdelast_driver_s::enqueue_step(int obs, int rebuild, cudaEvent_t const *ev) {
     int const grid = n_pad / kBlock;
     if (rebuild && neighbors) // calculate_neighbors() before integrate() (md.py:1245-1251)
         if (int rc = enqueue_rebuild())
@@ -724,8 +829,14 @@ int mdelast_driver_s::enqueue_step(int obs, int rebuild) {
         if (int rc = enqueue_rebuild())
             return rc;
     refresh_pair_list(stream);
+    if (ev)
+        CK(cudaEventRecord(ev[0], stream));
     pass_density(obs != 0, stream);
+    if (ev)
+        CK(cudaEventRecord(ev[1], stream));
     pass_force(obs != 0, true, stream);
+    if (ev)
+        CK(cudaEventRecord(ev[2], stream));
     post(POST_STEP, obs, stream);
     CK(cudaGetLastError());
     CK(cudaMemcpy2DAsync(h_obs, sizeof(mdelast_observables),
@@ -1814,6 +1925,31 @@ int mdelast_driver_autotune(mdelast_driver *d, int32_t n_repeat, int32_t *choice
     if (ms_out) {
         ms_out[0] = best_d;
         ms_out[1] = best_f;
+    }
+    return MDELAST_OK;
+}
+
+int mdelast_driver_autotune_steps(mdelast_driver *d, int32_t n_steps, int32_t rebuild_every,
+                                  int32_t *choice, double *ms_out) {
+    clear_error();
+    if (!d || n_steps < 1)
+        return fail(MDELAST_ERR_ARGUMENT, "bad argument");
+    CK(cudaSetDevice(d->device));
+    if (int rc = d->wait_step())
+        return rc;
+    if (d->neighbors && rebuild_every > 0)
+        if (int rc = d->configure_cells(d->current_boxes()))
+            return rc;
+    int c[4];
+    double ms[2];
+    if (int rc = d->tune_on_steps(n_steps, rebuild_every, c, ms))
+        return rc;
+    if (choice)
+        for (int k = 0; k < 4; ++k)
+            choice[k] = c[k];
+    if (ms_out) {
+        ms_out[0] = ms[0];
+        ms_out[1] = ms[1];
     }
     return MDELAST_OK;
 }

@@ -140,10 +140,13 @@ py::dict elastic_dict(mdelast_fluct const &f, int ensemble, double T, double P) 
     return out;
 }
 
-py::dict autotune_dict(mdelast_driver *d, int n_repeat) {
+py::dict autotune_dict(mdelast_driver *d, int n_repeat, int steps_rebuild = -1) {
     int32_t c[4];
     double ms[2];
-    check(mdelast_driver_autotune(d, n_repeat, c, ms));
+    if (steps_rebuild >= 0)
+        check(mdelast_driver_autotune_steps(d, n_repeat, steps_rebuild, c, ms));
+    else
+        check(mdelast_driver_autotune(d, n_repeat, c, ms));
     py::dict out;
     out["tpa_density"] = c[0];
     out["tpa_force"] = c[1];
@@ -558,6 +561,9 @@ class MDDriver {
     void synchronize() { check(mdelast_driver_synchronize(d_)); }
     void set_sample_ring(int capacity) { check(mdelast_driver_set_sample_ring(d_, capacity)); }
     py::dict autotune(int n_repeat) { return autotune_dict(d_, n_repeat); }
+    py::dict autotune_steps(int n, int rebuild_every) {
+        return autotune_dict(d_, n, rebuild_every);
+    }
     py::object force_staging() { return force_staging_get(d_); }
     py::tuple list_capacity() {
         int32_t m = 0, g = 0;
@@ -857,6 +863,9 @@ class BatchedMDDriver {
     // returns (gr, gr_partial) with gr_partial one row per type pair a <= b
     void set_sample_ring(int capacity) { check(mdelast_driver_set_sample_ring(d_, capacity)); }
     py::dict autotune(int n_repeat) { return autotune_dict(d_, n_repeat); }
+    py::dict autotune_steps(int n, int rebuild_every) {
+        return autotune_dict(d_, n, rebuild_every);
+    }
     py::object force_staging() { return force_staging_get(d_); }
     py::tuple list_capacity() {
         int32_t m = 0, g = 0;
@@ -1048,6 +1057,9 @@ PYBIND11_MODULE(md_driver_module, m) {
         .def("calculate_partial_pair_correlation", [](MDDriver &d) { d.pair_correlation(2); })
         .def("autotune", &MDDriver::autotune, py::arg("n_repeat") = 3,
              "time the pair passes over their launch shapes and keep the fastest")
+        .def("autotune_steps", &MDDriver::autotune_steps, py::arg("n_steps") = 4,
+             py::arg("rebuild_every") = 20,
+             "the same on real steps (the state advances by about 30 n_steps steps)")
         .def("set_launch", &MDDriver::set_launch, py::arg("tpa_density"), py::arg("tpa_force"),
              py::arg("blocks_density"), py::arg("blocks_force"))
         .def_property("force_staging", &MDDriver::force_staging, &MDDriver::set_force_staging,
@@ -1113,6 +1125,8 @@ PYBIND11_MODULE(md_driver_module, m) {
         .def("neighbor_list", &BatchedMDDriver::neighbor_list, py::arg("replica"))
         .def("kernel_times", &BatchedMDDriver::kernel_times, py::arg("n_steps") = 10)
         .def("autotune", &BatchedMDDriver::autotune, py::arg("n_repeat") = 3)
+        .def("autotune_steps", &BatchedMDDriver::autotune_steps, py::arg("n_steps") = 4,
+             py::arg("rebuild_every") = 20)
         .def("set_launch", &BatchedMDDriver::set_launch, py::arg("tpa_density"),
              py::arg("tpa_force"), py::arg("blocks_density"), py::arg("blocks_force"))
         .def_property("force_staging", &BatchedMDDriver::force_staging,
