@@ -71,21 +71,22 @@ EQUIL_STEPS = 400
 
 # ----------------------------------------------------------------------------- clocks
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms in the background."""
+    """nvidia-smi clocks and throttle reasons sampled every 20 ms in the background."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index):
+    def __init__(self, gpu_index, period_ms=20):
         self.gpu = gpu_index
+        self.period_ms = period_ms
         self.proc = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", str(self.period_ms)],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
@@ -118,7 +119,8 @@ class ClockSampler:
                 if f[5 + k].lower() == "active":
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "window": "warm-up and timed steps, every 20 ms"}
 
 
 # ----------------------------------------------------------------------------- ours
@@ -155,23 +157,28 @@ def run_ours(args, rank, world, local_rank):
     # larger than the 126 MB L2 for 16 replicas, so steps run back to back unflushed.
     b = make_batch(m, t, cells, dt=DT, r_skin=SKIN, precision=args.precision,
                    device=local_rank)
-    # launch shapes of the pair passes timed on this workload and kept (setup, untimed),
-    # or the shapes given by --launch
+    # equilibration from the lattice (untimed), then the launch shapes of the pair passes
+    # timed on this workload and kept, or the shapes given by --launch
+    b.run(EQUIL_STEPS, REBUILD, 1, False)
     if args.launch:
         tpa_d, tpa_f, blk_d, blk_f = (int(v) for v in args.launch.split(","))
         b.set_launch(tpa_d, tpa_f, blk_d, blk_f)
+        if args.force_tables != "auto" and b.force_staging is not None:
+            b.force_staging = args.force_tables == "shared"
         tune = {"tpa_density": tpa_d, "tpa_force": tpa_f, "blocks_density": blk_d,
-                "blocks_force": blk_f, "given": True}
+                "blocks_force": blk_f, "given": True, "force_staged": bool(b.force_staging)}
     else:
-        # equilibrate, then choose the shapes on real steps (the state advances)
-        b.run(EQUIL_STEPS, REBUILD, 1, False)
+        # shapes chosen on real steps (the state advances)
         tune = b.autotune_steps(TUNE_STEPS, REBUILD)
-    b.run(args.warmup, REBUILD, 1, False)
-    b.synchronize()
-    barrier()
+    # the sampler starts before the warm-up steps so that a short timed region still has
+    # samples (the timed steps follow the warm-up back to back)
     with ClockSampler(local_rank) as clk:
+        time.sleep(0.1)
+        b.run(args.warmup, REBUILD, 1, False)
+        b.synchronize()
+        barrier()
         ms_total = b.run(args.steps, REBUILD, 1, True)
-    barrier()
+        barrier()
     clocks = clk.summary()
     t_dev = torch.tensor([ms_total], dtype=torch.float64, device="cuda")
     if dist is not None:
@@ -191,8 +198,11 @@ def run_ours(args, rank, world, local_rank):
     roof = {"bound": "hbm", "kernel": "k_force" + ("_mx" if args.precision == "mixed" else ""),
             "achieved": achieved, "peak": peak, "unit": "GB/s",
             "peak_source": "measured" if hbm else "fallback", "frac": achieved / peak,
-            "traffic": TRAFFIC_PER_LAUNCH.get((args.precision, args.replicas))
+            "traffic": TRAFFIC_PER_LAUNCH.get((args.precision, args.replicas,
+                                               bool(tune.get("force_staged"))))
             if args.workload == WORKLOAD else None,
+            "traffic_source": "ncu single-pass capture at 16 replicas, caches not flushed",
+            "force_tables": "shared memory" if tune.get("force_staged") else "L1",
             "algorithmic_bytes_per_launch": bytes_force, "half_list_nbar": nbar,
             "kernel_ms": {n: float(x) for n, x in zip(KERNELS, kt)}}
     del b
@@ -294,8 +304,10 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0 and not args.no_e2e and args.workload == WORKLOAD:
         run_loop = dropin_run_loop(m, t)
     others = None if args.no_configs else other_configs(m, t, local_rank, peak=peak)
+    # per step: k_pre, k_kick_drift, k_sublist, density, force, k_reduce, k_post; per list
+    # rebuild: k_cell_bin, k_cell_sort, k_nbr_cells, k_nbr_build, k_sub_invalidate
     n_rebuilds = (args.steps + REBUILD - 1) // REBUILD
-    launches = args.steps * 6 + n_rebuilds * 3
+    launches = args.steps * 7 + n_rebuilds * 5
     line = {
         "metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_total / args.steps,
@@ -775,13 +787,13 @@ def half_list_nbar(m, t, cell):
     return float(point[-1]) / cell.n_atoms
 
 
-# ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_force_mx launch
-# (the capture of the bench command at 4 replicas summarised under profiles/, the 200th
-# step, cold caches); the 16- and 32-replica entries scale it by the atoms processed. None
-# where not captured.
-_TRAFFIC_4 = 39.520000e6 + 0.023296e6
-TRAFFIC_PER_LAUNCH: dict = {("mixed", 4): _TRAFFIC_4, ("mixed", 16): 4 * _TRAFFIC_4,
-                            ("mixed", 32): 8 * _TRAFFIC_4}
+# ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_force_mx launch, keyed by
+# (precision, replicas, staged tables): single-pass captures of the bench command at 16
+# replicas without cache flushing (the launches of timed-region steps, so the L2 holds
+# what the preceding kernels of the step left in it), mean over the captured launches;
+# profiles/launches_bench_mixed_16x13500.md has the capture. None where not captured.
+TRAFFIC_PER_LAUNCH: dict = {("mixed", 16, False): 81.30e6 + 0.80e6,
+                            ("mixed", 16, True): 77.74e6 + 0.43e6}
 
 
 # ----------------------------------------------------------------------------- reference
@@ -876,6 +888,9 @@ def main():
     ap.add_argument("--launch", default=None, metavar="TPA_D,TPA_F,BLOCKS_D,BLOCKS_F",
                     help="launch shapes of the density and force passes instead of the "
                          "autotuner's (lanes per atom, target block count)")
+    ap.add_argument("--force-tables", choices=("auto", "l1", "shared"), default="auto",
+                    help="with --launch: the force pass reads its tables through the L1 or "
+                         "from the staged shared-memory copy (default: as the driver has it)")
     ap.add_argument("--workload", choices=tuple(WORKLOADS), default=WORKLOAD,
                     help="the timed batch's cell (the C_ij comparisons always use the "
                          "Cu-Zn cell)")
