@@ -111,9 +111,9 @@ constexpr int kTargetBlocks = 148 * 32;
 // shared memory for the staged force tables: beside it the kernel keeps its FP64
 // accumulators (40 KB at 4 lanes per atom) within the 227 KB a block may take
 constexpr long kStageBudget = 184 * 1024;
-// k_sublist grid: one wave, 4 resident blocks of 256 threads (48 registers each) on each of
-// the 148 SMs
-constexpr int kSublistBlocks = 148 * 4;
+// k_sublist grid: one wave, 5 resident blocks of 256 threads (48 registers each: 5 blocks
+// fill the register file) on each of the 148 SMs
+constexpr int kSublistBlocks = 148 * 5;
 
 int deal_blocks(std::vector<Replica *> const &reps, int tpa, bool density,
                 std::vector<int> &blk_rep, int target = kTargetBlocks,
