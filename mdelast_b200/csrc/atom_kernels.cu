@@ -477,174 +477,246 @@ __global__ void __launch_bounds__(kBlock) k_density(AtomsView A, TablesView T) {
 // Global sums (virial, Born stress, Born tensor, pair Laplacian) take each pair once, on
 // its j > i visit; the Born tensor is accumulated as the 15 distinct degree-4 monomials
 // X p_a p_b p_c p_d of which its 21 upper-triangle entries are made.
+//
+// Each atom row is walked in two loops, partners j > i (which also feed the global sums)
+// and partners j < i, so the lanes of a warp do not diverge on the global-sum work. A
+// row's global sums are summed in FP64 registers along the row and added, once per atom
+// and combined across its TPA lanes, into FP64 block accumulators in shared memory, one
+// set per lane group: the loops then keep 23 FP64 sums live instead of all 35 of the block,
+// and three 128-thread blocks of the observable-step variant fit an SM instead of two.
+
+template <bool OBS> struct RowSums64 {
+    double virial = 0.;
+    double sig[6] = {0., 0., 0., 0., 0., 0.};
+    double cb[OBS ? 15 : 1] = {};
+    double lap = 0.;
+};
+
+struct RowIn64 {
+    double4 ci;
+    double dFi, d2Fi;
+    int ti;
+    double hx, hy, hz;
+};
+
+template <bool OBS, bool UPPER, int TPA, int IP, typename IX>
+__device__ __forceinline__ void force_row(AtomsView const &A, TablesView const &T,
+                                          RowIn64 const &in, PairRow<IX> const &row, int n,
+                                          int sub, double &fx, double &fy, double &fz,
+                                          double &epot, RowSums64<OBS> &ps, bool &warn_rmin) {
+    constexpr int kF = TabFmt<IP>::kF;
+    if (sub >= n)
+        return;
+    auto slot = [&](int k) { return UPPER ? k : A.pmaxn - 1 - k; };
+    int const ti = in.ti;
+    double const dFi = in.dFi, d2Fi = in.d2Fi;
+    // the next partner's index, record and F' are loaded one iteration ahead
+    int jn = row.at(slot(sub));
+    double4 cn = A.crd[jn];
+    double2 fn = A.dF2[jn];
+    for (int kk = sub; kk < n; kk += TPA) {
+        double4 const cj = cn;
+        double2 const dFj2 = fn;
+        if (kk + TPA < n) {
+            jn = row.at(slot(kk + TPA));
+            cn = A.crd[jn];
+            fn = A.dF2[jn];
+        }
+        double px, py, pz;
+        double const r2 = min_image_r2(in.ci, cj, in.hx, in.hy, in.hz, px, py, pz);
+        if (r2 > T.r_cut_sq)
+            continue;
+        double const dr = sqrt(r2);
+        double const idr = 1. / dr;
+        int const tj = static_cast<int>(cj.w);
+        int const s = pair_slot(ti, tj);
+        double t;
+        int const k = tab_locate(dr, T.inv_hr, T.nri, t);
+        const double *bundle = T.rb + (static_cast<size_t>(s) * T.nri + k) * 3 * kF;
+        // TablePotential::calculate (potential.hpp:92-104)
+        double V = 0., dV = 0., d2V = 0.;
+        if (dr < T.pot_rmin[s])
+            warn_rmin = true;
+        if (!(dr > T.pot_rcut[s]))
+            tab_eval<IP, true, true, OBS && UPPER>(bundle, t, T.inv_hr, T.inv_hr2, V, dV, d2V);
+        double dedr = dV;
+        double X = 0., lap = 0.;
+        if (OBS && UPPER) {
+            X = d2V - dV * idr;
+            lap = 2. * (d2V + 2. * dV * idr);
+        }
+        if (T.has_eam) {
+            // rho of the lower type at bundle offset kF, of the higher type at 2 kF
+            int const oi = (ti <= tj) ? kF : 2 * kF, oj = (ti < tj) ? 2 * kF : kF;
+            double drho_i = 0., drho_j = 0., d2rho_i = 0., d2rho_j = 0., unused = 0.;
+            if (!(dr > T.eam_rcut[ti]))
+                tab_eval<IP, false, true, OBS && UPPER>(bundle + oi, t, T.inv_hr, T.inv_hr2,
+                                                        unused, drho_i, d2rho_i);
+            if (!(dr > T.eam_rcut[tj]))
+                tab_eval<IP, false, true, OBS && UPPER>(bundle + oj, t, T.inv_hr, T.inv_hr2,
+                                                        unused, drho_j, d2rho_j);
+            double const dFj = dFj2.x;
+            // the two cross terms are rounded separately and added (commutative), so
+            // the i- and j-side evaluations of dE/dr are bitwise equal
+            dedr = __dadd_rn(dedr, __dadd_rn(__dmul_rn(dFi, drho_j), __dmul_rn(dFj, drho_i)));
+            if (OBS && UPPER) {
+                double const d2Fj = dFj2.y;
+                lap += 2. * (dFj * (d2rho_i + 2. * drho_i * idr) +
+                             dFi * (d2rho_j + 2. * drho_j * idr));
+                lap += d2Fi * (drho_j * drho_j) + d2Fj * (drho_i * drho_i);
+                X += dFi * (d2rho_j - drho_j * idr) + dFj * (d2rho_i - drho_i * idr);
+            }
+        }
+        double const sc = __dmul_rn(-dedr, idr);
+        fx += __dmul_rn(sc, px);
+        fy += __dmul_rn(sc, py);
+        fz += __dmul_rn(sc, pz);
+        epot += 0.5 * V;
+        if (UPPER) {
+            ps.virial += dr * dedr;
+            double const xx = px * px, yy = py * py, zz = pz * pz;
+            double const yz = py * pz, xz = px * pz, xy = px * py;
+            double const w = dedr * idr;
+            ps.sig[0] += w * xx;
+            ps.sig[1] += w * yy;
+            ps.sig[2] += w * zz;
+            ps.sig[3] += w * yz;
+            ps.sig[4] += w * xz;
+            ps.sig[5] += w * xy;
+            if (OBS) {
+                X *= idr * idr;
+                double const Xxx = X * xx, Xyy = X * yy, Xzz = X * zz;
+                ps.cb[0] += Xxx * xx;  // x4
+                ps.cb[1] += Xyy * yy;  // y4
+                ps.cb[2] += Xzz * zz;  // z4
+                ps.cb[3] += Xxx * xy;  // x3y
+                ps.cb[4] += Xxx * xz;  // x3z
+                ps.cb[5] += Xyy * xy;  // xy3
+                ps.cb[6] += Xyy * yz;  // y3z
+                ps.cb[7] += Xzz * xz;  // xz3
+                ps.cb[8] += Xzz * yz;  // yz3
+                ps.cb[9] += Xxx * yy;  // x2y2
+                ps.cb[10] += Xxx * zz; // x2z2
+                ps.cb[11] += Xyy * zz; // y2z2
+                ps.cb[12] += Xxx * yz; // x2yz
+                ps.cb[13] += Xyy * xz; // xy2z
+                ps.cb[14] += Xzz * xy; // xyz2
+                ps.lap += lap;
+            }
+        }
+    }
+}
 
 template <bool OBS, bool KICK, int TPA, int IP, typename IX>
 __global__ void __launch_bounds__(kBlock) k_force(AtomsView A, TablesView T) {
     if (halted(A)) // a list build ran out of capacity: nothing until the host regrows
         return;
-    constexpr int kF = TabFmt<IP>::kF;
+    constexpr int kG = kBlock / TPA;
+    __shared__ double s_acc[F_NSUM * kG];
+    int const tid = threadIdx.x, grp = tid / TPA;
+    for (int k = tid; k < F_NSUM * kG; k += kBlock)
+        s_acc[k] = 0.;
+    __syncthreads();
     int const r = A.fblk_rep[blockIdx.x];
     Replica const *R = A.rep + r;
     int const lb = blockIdx.x - R->fblk_begin, nb = R->fblk_n;
-    int const apb = kBlock / TPA, sub = threadIdx.x % TPA;
+    int const apb = kBlock / TPA, sub = tid % TPA;
     int const n_slots = R->n_blocks * kBlock;
-    double const hx = R->h[0], hy = R->h[1], hz = R->h[2];
+    RowIn64 in;
+    in.hx = R->h[0];
+    in.hy = R->h[1];
+    in.hz = R->h[2];
+    for (int a0 = lb * apb; a0 < n_slots; a0 += nb * apb) {
+        int const a = a0 + tid / TPA;
+        int const i = R->atom_begin + a;
+        bool const valid = a < R->n_atoms;
+        double fx = 0., fy = 0., fz = 0., epot = 0.;
+        double sums[F_F2]; // this atom's pair sums (virial, Born stress, tensor, Laplacian)
+#pragma unroll
+        for (int k = 0; k < F_F2; ++k)
+            sums[k] = 0.;
+        in.ti = 0;
+        if (valid) {
+            in.ci = A.crd[i];
+            in.ti = static_cast<int>(in.ci.w);
+            double2 const dFi2 = T.has_eam ? A.dF2[i] : make_double2(0., 0.);
+            in.dFi = dFi2.x;
+            in.d2Fi = OBS ? dFi2.y : 0.;
+            int const nu = A.pn_up[i], nd = A.pn_dn[i];
+            PairRow<IX> const row = pair_row<IX>(A, i, R->atom_begin);
+            bool warn_rmin = false;
+            RowSums64<OBS> ps;
+            force_row<OBS, true, TPA, IP, IX>(A, T, in, row, nu, sub, fx, fy, fz, epot, ps,
+                                              warn_rmin);
+            force_row<OBS, false, TPA, IP, IX>(A, T, in, row, nd, sub, fx, fy, fz, epot, ps,
+                                               warn_rmin);
+            if (warn_rmin)
+                status_or(A.rep + r, MDELAST_WARN_RMIN);
+            sums[F_VIRIAL] = ps.virial;
+#pragma unroll
+            for (int k = 0; k < 6; ++k)
+                sums[F_SIGMA + k] = ps.sig[k];
+            if (OBS) {
+#pragma unroll
+                for (int k = 0; k < 15; ++k)
+                    sums[F_CB + k] = ps.cb[k];
+                sums[F_LAP] = ps.lap;
+            }
+        }
+        fx = group_sum<TPA>(fx);
+        fy = group_sum<TPA>(fy);
+        fz = group_sum<TPA>(fz);
+        epot = group_sum<TPA>(epot);
+        constexpr int kPair = OBS ? F_F2 : F_CB; // the pair sums this step forms
+#pragma unroll
+        for (int k = 0; k < kPair; ++k)
+            sums[k] = group_sum<TPA>(sums[k]);
+        if (sub == 0) {
+#pragma unroll
+            for (int k = 0; k < kPair; ++k)
+                s_acc[k * kG + grp] += sums[k];
+        }
+        if (valid && sub == 0) {
+            if (T.has_eam)
+                epot += A.Fe[i];
+            size_t const np = A.n_pad;
+            A.frc[i] = fx;
+            A.frc[np + i] = fy;
+            A.frc[np + i + np] = fz;
+            A.epot[i] = epot;
+            double const m = T.mass[in.ti];
+            double vx = A.vel[i], vy = A.vel[np + i], vz = A.vel[2 * np + i];
+            if (KICK) {
+                // U2 (md_driver.cpp:446-449): v = v e + (c dt) F / m
+                double const e = R->e_kick, cdt = R->cdt_kick;
+                vx = vx * e + cdt * fx / m;
+                vy = vy * e + cdt * fy / m;
+                vz = vz * e + cdt * fz / m;
+                A.vel[i] = vx;
+                A.vel[np + i] = vy;
+                A.vel[2 * np + i] = vz;
+            }
+            double *acc = s_acc + grp;
+            acc[F_F2 * kG] += fx * fx + fy * fy + fz * fz;
+            acc[F_EKIN * kG] += 0.5 * m * (vx * vx + vy * vy + vz * vz);
+            acc[(F_MVV + 0) * kG] += m * vx * vx;
+            acc[(F_MVV + 1) * kG] += m * vy * vy;
+            acc[(F_MVV + 2) * kG] += m * vz * vz;
+            acc[(F_MVV + 3) * kG] += m * vy * vz;
+            acc[(F_MVV + 4) * kG] += m * vx * vz;
+            acc[(F_MVV + 5) * kG] += m * vx * vy;
+            acc[(F_MV + 0) * kG] += vx * m;
+            acc[(F_MV + 1) * kG] += vy * m;
+            acc[(F_MV + 2) * kG] += vz * m;
+            acc[F_EPOT * kG] += epot;
+        }
+    }
+    // the groups' slots into the block sums
+    __syncthreads();
     double acc[F_NSUM];
 #pragma unroll
     for (int k = 0; k < F_NSUM; ++k)
-        acc[k] = 0.;
-    for (int a0 = lb * apb; a0 < n_slots; a0 += nb * apb) {
-    int const a = a0 + static_cast<int>(threadIdx.x) / TPA;
-    int const i = R->atom_begin + a;
-    bool const valid = a < R->n_atoms;
-    double fx = 0., fy = 0., fz = 0., epot = 0.;
-    double4 ci = make_double4(0., 0., 0., 0.);
-    if (valid) {
-        ci = A.crd[i];
-        int const ti = static_cast<int>(ci.w);
-        double2 const dFi2 = T.has_eam ? A.dF2[i] : make_double2(0., 0.);
-        double const dFi = dFi2.x, d2Fi = OBS ? dFi2.y : 0.;
-        int const nu = A.pn_up[i], ntot = nu + A.pn_dn[i];
-        PairRow<IX> const row = pair_row<IX>(A, i, R->atom_begin);
-        bool warn_rmin = false;
-        // the next partner's index, record and F' are loaded one iteration ahead
-        int jn = sub < ntot ? row.at(list_slot(sub, nu, A.pmaxn)) : i;
-        double4 cn = A.crd[jn];
-        double2 fn = A.dF2[jn];
-        for (int kk = sub; kk < ntot; kk += TPA) {
-            bool const upper = kk < nu;
-            double4 const cj = cn;
-            double2 const dFj2 = fn;
-            if (kk + TPA < ntot) {
-                jn = row.at(list_slot(kk + TPA, nu, A.pmaxn));
-                cn = A.crd[jn];
-                fn = A.dF2[jn];
-            }
-            double px, py, pz;
-            double const r2 = min_image_r2(ci, cj, hx, hy, hz, px, py, pz);
-            if (r2 > T.r_cut_sq)
-                continue;
-            double const dr = sqrt(r2);
-            double const idr = 1. / dr;
-            int const tj = static_cast<int>(cj.w);
-            int const s = pair_slot(ti, tj);
-            double t;
-            int const k = tab_locate(dr, T.inv_hr, T.nri, t);
-            const double *bundle = T.rb + (static_cast<size_t>(s) * T.nri + k) * 3 * kF;
-            // TablePotential::calculate (potential.hpp:92-104)
-            double V = 0., dV = 0., d2V = 0.;
-            if (dr < T.pot_rmin[s])
-                warn_rmin = true;
-            if (!(dr > T.pot_rcut[s]))
-                tab_eval<IP, true, true, OBS>(bundle, t, T.inv_hr, T.inv_hr2, V, dV, d2V);
-            double dedr = dV;
-            double X = 0., lap = 0.;
-            if (OBS) {
-                X = d2V - dV * idr;
-                lap = 2. * (d2V + 2. * dV * idr);
-            }
-            if (T.has_eam) {
-                // rho of the lower type at bundle offset kF, of the higher type at 2 kF
-                int const oi = (ti <= tj) ? kF : 2 * kF, oj = (ti < tj) ? 2 * kF : kF;
-                double drho_i = 0., drho_j = 0., d2rho_i = 0., d2rho_j = 0., unused = 0.;
-                if (!(dr > T.eam_rcut[ti]))
-                    tab_eval<IP, false, true, OBS>(bundle + oi, t, T.inv_hr, T.inv_hr2, unused,
-                                                   drho_i, d2rho_i);
-                if (!(dr > T.eam_rcut[tj]))
-                    tab_eval<IP, false, true, OBS>(bundle + oj, t, T.inv_hr, T.inv_hr2, unused,
-                                                   drho_j, d2rho_j);
-                double const dFj = dFj2.x;
-                // the two cross terms are rounded separately and added (commutative), so
-                // the i- and j-side evaluations of dE/dr are bitwise equal
-                dedr = __dadd_rn(dedr, __dadd_rn(__dmul_rn(dFi, drho_j), __dmul_rn(dFj, drho_i)));
-                if (OBS) {
-                    double const d2Fj = dFj2.y;
-                    lap += 2. * (dFj * (d2rho_i + 2. * drho_i * idr) +
-                                 dFi * (d2rho_j + 2. * drho_j * idr));
-                    lap += d2Fi * (drho_j * drho_j) + d2Fj * (drho_i * drho_i);
-                    X += dFi * (d2rho_j - drho_j * idr) + dFj * (d2rho_i - drho_i * idr);
-                }
-            }
-            double const sc = __dmul_rn(-dedr, idr);
-            fx += __dmul_rn(sc, px);
-            fy += __dmul_rn(sc, py);
-            fz += __dmul_rn(sc, pz);
-            epot += 0.5 * V;
-            if (upper) {
-                acc[F_VIRIAL] += dr * dedr;
-                double const xx = px * px, yy = py * py, zz = pz * pz;
-                double const yz = py * pz, xz = px * pz, xy = px * py;
-                double const w = dedr * idr;
-                acc[F_SIGMA + 0] += w * xx;
-                acc[F_SIGMA + 1] += w * yy;
-                acc[F_SIGMA + 2] += w * zz;
-                acc[F_SIGMA + 3] += w * yz;
-                acc[F_SIGMA + 4] += w * xz;
-                acc[F_SIGMA + 5] += w * xy;
-                if (OBS) {
-                    X *= idr * idr;
-                    double const Xxx = X * xx, Xyy = X * yy, Xzz = X * zz;
-                    acc[F_CB + 0] += Xxx * xx;  // x4
-                    acc[F_CB + 1] += Xyy * yy;  // y4
-                    acc[F_CB + 2] += Xzz * zz;  // z4
-                    acc[F_CB + 3] += Xxx * xy;  // x3y
-                    acc[F_CB + 4] += Xxx * xz;  // x3z
-                    acc[F_CB + 5] += Xyy * xy;  // xy3
-                    acc[F_CB + 6] += Xyy * yz;  // y3z
-                    acc[F_CB + 7] += Xzz * xz;  // xz3
-                    acc[F_CB + 8] += Xzz * yz;  // yz3
-                    acc[F_CB + 9] += Xxx * yy;  // x2y2
-                    acc[F_CB + 10] += Xxx * zz; // x2z2
-                    acc[F_CB + 11] += Xyy * zz; // y2z2
-                    acc[F_CB + 12] += Xxx * yz; // x2yz
-                    acc[F_CB + 13] += Xyy * xz; // xy2z
-                    acc[F_CB + 14] += Xzz * xy; // xyz2
-                    acc[F_LAP] += lap;
-                }
-            }
-        }
-        if (warn_rmin)
-            status_or(A.rep + r, MDELAST_WARN_RMIN);
-    }
-    fx = group_sum<TPA>(fx);
-    fy = group_sum<TPA>(fy);
-    fz = group_sum<TPA>(fz);
-    epot = group_sum<TPA>(epot);
-    if (valid && sub == 0) {
-        int const ti = static_cast<int>(ci.w);
-        if (T.has_eam)
-            epot += A.Fe[i];
-        size_t const np = A.n_pad;
-        A.frc[i] = fx;
-        A.frc[np + i] = fy;
-        A.frc[np + i + np] = fz;
-        A.epot[i] = epot;
-        double const m = T.mass[ti];
-        double vx = A.vel[i], vy = A.vel[np + i], vz = A.vel[2 * np + i];
-        if (KICK) {
-            // U2 (md_driver.cpp:446-449): v = v e + (c dt) F / m
-            double const e = R->e_kick, cdt = R->cdt_kick;
-            vx = vx * e + cdt * fx / m;
-            vy = vy * e + cdt * fy / m;
-            vz = vz * e + cdt * fz / m;
-            A.vel[i] = vx;
-            A.vel[np + i] = vy;
-            A.vel[2 * np + i] = vz;
-        }
-        acc[F_F2] += fx * fx + fy * fy + fz * fz;
-        acc[F_EKIN] += 0.5 * m * (vx * vx + vy * vy + vz * vz);
-        acc[F_MVV + 0] += m * vx * vx;
-        acc[F_MVV + 1] += m * vy * vy;
-        acc[F_MVV + 2] += m * vz * vz;
-        acc[F_MVV + 3] += m * vy * vz;
-        acc[F_MVV + 4] += m * vx * vz;
-        acc[F_MVV + 5] += m * vx * vy;
-        acc[F_MV + 0] += vx * m;
-        acc[F_MV + 1] += vy * m;
-        acc[F_MV + 2] += vz * m;
-        acc[F_EPOT] += epot;
-    }
-    }
+        acc[k] = tid < kG ? s_acc[k * kG + tid] : 0.;
     block_sum_store<F_NSUM>(acc, A.pf + static_cast<size_t>(blockIdx.x) * F_NSUM);
 }
 
