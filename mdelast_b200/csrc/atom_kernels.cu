@@ -12,12 +12,15 @@ namespace mdelast {
 // ------------------------------------------------------------------------------------
 // neighbour list (md_driver.cpp:279-298): every pair with the reference's min-image
 // |p|^2 <= (rcut r_skin)^2, found through a cell list (or all pairs when a replica has
-// fewer than 3 cells along an edge). The cell grid is fixed when a run starts; a barostat
+// fewer than 3 list radii along an edge). Atoms are binned into half cells: 2 nc per edge
+// for the nc = floor(h / (1.05 r_list)) cells no thinner than the list radius (with a margin
+// for the box changes of an NPT run between rebuilds), so the partners of an atom lie in
+// the 5 x 5 x 5 half cells around its own. The grid is fixed when a run starts; a barostat
 // may shrink the box below it between builds, so each build takes, along every edge, the
-// reach k (cells either side) with k * h / nc >= the list radius in the current box.
+// reach k (half cells either side) with k * h / nc >= the list radius in the current box.
 
-// reach along one edge of h with nc cells (1 while the cells are no narrower than the
-// list radius, as they start)
+// reach along one edge of h with nc (half) cells (2 while two half cells span the list
+// radius, as they start)
 __device__ __forceinline__ int cell_reach(double h, int nc, double rl2) {
     double const w = h / nc;
     int k = 1;
@@ -34,9 +37,15 @@ __device__ __forceinline__ void cell_span(int idx, int nc, int k, int &first, in
     first = fits ? idx - k : 0;
 }
 
+// the box has shrunk so far that two half cells no longer span the list radius (reach > 2
+// along some edge; written without divisions, with a relative slack of 1e-12 towards
+// calling the cells narrow)
 __device__ __forceinline__ bool narrow_cells(Replica const &R, double rl2) {
-    return cell_reach(R.h[0], R.nc[0], rl2) > 1 || cell_reach(R.h[1], R.nc[1], rl2) > 1 ||
-           cell_reach(R.h[2], R.nc[2], rl2) > 1;
+    bool n = false;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+        n = n || (R.nc[a] > 2 && 4. * R.h[a] * R.h[a] <= rl2 * R.nc[a] * R.nc[a] * (1. + 1e-12));
+    return n;
 }
 
 __global__ void k_cell_bin(AtomsView A) {
@@ -68,21 +77,32 @@ __global__ void k_cell_bin(AtomsView A) {
 }
 
 // Order each cell's members by slot index (rank sort in shared memory), so that the list
-// and everything summed over it are deterministic.
+// and everything summed over it are deterministic. One warp per half cell (about 8 atoms),
+// kCellSortWarps cells per block.
 __global__ void k_cell_sort(AtomsView A) {
     extern __shared__ int s_mem[];
-    int const cell = blockIdx.x;
-    int n = A.cell_count[cell];
+    __shared__ int s_max; // the block's largest cell count: one global atomic per block
+    int const lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int const cell = blockIdx.x * kCellSortWarps + warp;
+    if (threadIdx.x == 0)
+        s_max = 0;
+    __syncthreads();
+    int n = cell < A.n_cells ? A.cell_count[cell] : 0;
+    if (lane == 0)
+        atomicMax(&s_max, n);
+    __syncthreads();
+    if (threadIdx.x == 0)
+        atomicMax(&A.max_count[1], s_max);
+    if (cell >= A.n_cells)
+        return;
     if (n > A.cell_cap)
         n = A.cell_cap;
-    if (threadIdx.x == 0)
-        atomicMax(&A.max_count[1], A.cell_count[cell]);
-    int *src = s_mem;
+    int *src = s_mem + static_cast<size_t>(warp) * A.cell_cap;
     int *dst = A.cell_atoms + static_cast<size_t>(cell) * A.cell_cap;
-    for (int k = threadIdx.x; k < n; k += blockDim.x)
+    for (int k = lane; k < n; k += 32)
         src[k] = dst[k];
-    __syncthreads();
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    __syncwarp();
+    for (int k = lane; k < n; k += 32) {
         int const v = src[k];
         int rank = 0;
         for (int m = 0; m < n; ++m)
@@ -118,135 +138,256 @@ __device__ __forceinline__ void nb_batch(AtomsView const &A, int i, int j, bool 
     nd += cd;
 }
 
-// Cell-list replicas: one block per cell. The partners of the cell's atoms all lie in its
-// 27 stencil cells, so their records are staged in shared memory once per cell (in chunks
-// of kStage, in the stencil order dz, dy, dx and member order of the per-atom search below)
-// and each warp tests its atoms against the staged records: the same candidates in the same
-// order as the per-atom search, so the same list, without re-gathering every candidate
-// from global memory for each atom of the cell. Replicas whose box has shrunk below the
-// cell grid (reach > 1) are left to k_nbr_build.
+// Cell-list replicas: one block per group of 2 x 2 x 2 half cells (one cell of the
+// coarse grid). The partners of the group's atoms all lie in the 6 x 6 x 6 half cells
+// around it (its window), so their records are staged in shared memory once per group
+// (in chunks of kStageH, window cells in z, y, x order, members in slot order) and each
+// warp tests one atom at a time against them. An atom's partners lie in the 5 x 5 x 5 half
+// cells around its own, and of those only the cells its list sphere reaches: per row of
+// five half cells along x (fixed z, y) the warp takes the lower bound of the distance from
+// the atom to the row, skips rows beyond the radius and trims the row's x range to the
+// cells within it; each trimmed row is a contiguous run of staged records. On the 13,500-atom
+// Cu-Zn cell that tests about 510 candidates per atom instead of the window's 1,690.
 //
-// Most staged candidates (about 7 in 8) lie well outside the list radius. Each is first
-// tested in FP32 on wrapped scaled coordinates with a margin that covers the FP32 error
-// (so no pair within the radius is dropped); the survivors are packed, in candidate order,
-// into a per-warp queue and get the reference's exact FP64 test 32 at a time, with every
-// lane busy. The pairs kept and their order are those of the plain FP64 search.
-constexpr int kStage = 512;
-constexpr int kWarps = 4; // warps per block of k_nbr_cells
+// Each candidate is first tested in FP32 on positions in the group's frame with a margin
+// that covers the FP32 error, from outside (no pair within the radius is dropped) and from
+// inside (a pair well within it needs no further test); the survivors are packed, in
+// candidate order, into a per-warp queue, stored 32 at a time, and the few that lie within
+// the error margin of the radius get the reference's exact FP64 test first. Rows, runs and
+// members come in a fixed order, so the list is deterministic; the pairs kept are exactly
+// those of the all-pairs search.
+constexpr int kStageH = 2048;
+constexpr int kWarpsH = kNbrCellsThreads / 32; // warps per block of k_nbr_cells
+constexpr int kWin = 6;    // window edge, half cells
+constexpr int kNearEdge = 1 << 30; // queue flag: the candidate needs the FP64 test
 
-__global__ void __launch_bounds__(128) k_nbr_cells(AtomsView A) {
+// lower bound (in half-cell widths) of the distance along one edge from an atom at
+// fraction f of its half cell to the half cell d cells away; a small slack keeps the bound
+// below the true distance under the FP32 rounding of f
+__device__ __forceinline__ float cell_gap(int d, float f) {
+    float const g = d > 0 ? static_cast<float>(d) - f
+                          : (d < 0 ? static_cast<float>(-d - 1) + f : 0.f);
+    return fmaxf(g - 1e-3f, 0.f);
+}
+
+__global__ void __launch_bounds__(kWarpsH * 32, 3) k_nbr_cells(AtomsView A) {
     extern __shared__ unsigned char s_raw[];
-    double4 *s_c = reinterpret_cast<double4 *>(s_raw);
-    float4 *s_w = reinterpret_cast<float4 *>(s_c + kStage); // wrapped scaled, FP32
-    int *s_j = reinterpret_cast<int *>(s_w + kStage);
-    int *s_cnt = s_j + kStage;    // [4][cell_cap]: nu, nd, total, full of the cell's atoms
-    __shared__ int s_cell[27], s_off[28];
-    __shared__ int s_queue[kWarps][64]; // staged indices that passed the FP32 test
-    int const cell = blockIdx.x;
-    int const r = A.cell_rep[cell];
+    float4 *s_w = reinterpret_cast<float4 *>(s_raw); // wrapped scaled, FP32
+    int *s_j = reinterpret_cast<int *>(s_w + kStageH);
+    int const cap = A.cell_cap, me_cap = 8 * cap;
+    int *s_me = s_j + kStageH; // the group's atoms
+    int *s_mq = s_me + me_cap; // ... and the window cell of each
+    int *s_cnt = s_mq + me_cap; // [4][me_cap]: nu, nd, total, full of the group's atoms
+    __shared__ int s_cell[kWin * kWin * kWin], s_off[kWin * kWin * kWin + 1], s_moff[9];
+    __shared__ int s_tmax; // the group's largest neighbour count
+    __shared__ int s_queue[kWarpsH][64]; // staged indices that passed the FP32 test
+    int const r = A.cell_rep[8 * blockIdx.x];
     Replica const &R = A.rep[r];
     if (narrow_cells(R, A.r_list_sq))
         return;
-    int const loc = cell - R.cell_begin;
-    int const cx0 = loc % R.nc[0], cy0 = (loc / R.nc[0]) % R.nc[1],
-              cz0 = loc / (R.nc[0] * R.nc[1]);
-    int const cap = A.cell_cap;
-    int const n_me = min(A.cell_count[cell], cap);
-    int const *me = A.cell_atoms + static_cast<size_t>(cell) * cap;
-    int *c_nu = s_cnt, *c_nd = s_cnt + cap, *c_tot = s_cnt + 2 * cap, *c_full = s_cnt + 3 * cap;
-    for (int a = threadIdx.x; a < n_me; a += blockDim.x)
-        c_nu[a] = c_nd[a] = c_tot[a] = c_full[a] = 0;
-    if (threadIdx.x == 0) {
-        int q = 0, off = 0;
-        for (int dz = -1; dz <= 1; ++dz) {
-            int const cz = (cz0 + dz + R.nc[2]) % R.nc[2];
-            for (int dy = -1; dy <= 1; ++dy) {
-                int const cy = (cy0 + dy + R.nc[1]) % R.nc[1];
-                for (int dx = -1; dx <= 1; ++dx, ++q) {
-                    int const cx = (cx0 + dx + R.nc[0]) % R.nc[0];
-                    int const c = R.cell_begin + (cz * R.nc[1] + cy) * R.nc[0] + cx;
-                    s_cell[q] = c;
-                    s_off[q] = off;
-                    off += min(A.cell_count[c], cap);
-                }
-            }
-        }
-        s_off[27] = off;
+    int const nx = R.nc[0], ny = R.nc[1], nz = R.nc[2];
+    int const grp = blockIdx.x - R.cell_begin / 8;
+    int const gx = grp % (nx / 2), gy = (grp / (nx / 2)) % (ny / 2),
+              gz = grp / ((nx / 2) * (ny / 2));
+    constexpr int kCells = kWin * kWin * kWin;
+    for (int q = threadIdx.x; q < kCells; q += blockDim.x) {
+        int const u = q % kWin, v = (q / kWin) % kWin, w = q / (kWin * kWin);
+        int const cx = (2 * gx - 2 + u + nx) % nx, cy = (2 * gy - 2 + v + ny) % ny,
+                  cz = (2 * gz - 2 + w + nz) % nz;
+        int const c = R.cell_begin + (cz * ny + cy) * nx + cx;
+        s_cell[q] = c;
+        s_off[q + 1] = min(A.cell_count[c], cap);
     }
     __syncthreads();
-    int const M = s_off[27];
     unsigned const lane = threadIdx.x & 31u;
     int const warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    unsigned const lt = (1u << lane) - 1u;
+    if (warp == 0) {
+        // exclusive scan of the window cells' counts; the group's 8 cells' counts
+        int carry = 0;
+        for (int b = 0; b < kCells; b += 32) {
+            int const q = b + static_cast<int>(lane);
+            int const c = q < kCells ? s_off[q + 1] : 0;
+            int incl = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int const t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (static_cast<int>(lane) >= o)
+                    incl += t;
+            }
+            if (q < kCells)
+                s_off[q + 1] = carry + incl;
+            carry += __shfl_sync(0xffffffffu, incl, 31);
+        }
+        if (lane == 0)
+            s_off[0] = 0;
+        __syncwarp();
+        // the group's cells are the window cells with u, v, w in {2, 3}
+        int const k = static_cast<int>(lane) & 7;
+        int const q = ((2 + (k >> 2)) * kWin + 2 + ((k >> 1) & 1)) * kWin + 2 + (k & 1);
+        int const c = s_off[q + 1] - s_off[q];
+        int incl = c;
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1) {
+            int const t = __shfl_up_sync(0xffffffffu, incl, o);
+            if ((static_cast<int>(lane) & 7) >= o)
+                incl += t;
+        }
+        if (lane < 8)
+            s_moff[k + 1] = incl;
+        if (lane == 0) {
+            s_moff[0] = 0;
+            s_tmax = 0;
+        }
+    }
+    __syncthreads();
+    int const n_me = s_moff[8];
+    for (int a = threadIdx.x; a < n_me; a += blockDim.x) {
+        int k = 0;
+        while (s_moff[k + 1] <= a)
+            ++k;
+        int const q = ((2 + (k >> 2)) * kWin + 2 + ((k >> 1) & 1)) * kWin + 2 + (k & 1);
+        s_me[a] = A.cell_atoms[static_cast<size_t>(s_cell[q]) * cap + (a - s_moff[k])];
+        s_mq[a] = q;
+    }
+    int *c_nu = s_cnt, *c_nd = s_cnt + me_cap, *c_tot = s_cnt + 2 * me_cap,
+        *c_full = s_cnt + 3 * me_cap;
+    for (int a = threadIdx.x; a < n_me; a += blockDim.x)
+        c_nu[a] = c_nd[a] = c_tot[a] = c_full[a] = 0;
+    int const M = s_off[kCells];
     double const hx = R.h[0], hy = R.h[1], hz = R.h[2];
     double const rl2 = A.r_list_sq;
-    // FP32 pre-test: |w| <= 1/2 carries at most 2^-26 of rounding per coordinate, the
-    // difference at most 3 2^-26 before the scaling by h; 1e-7 (h_x + h_y + h_z) and a
-    // 1e-6 relative widening of the radius cover that and the FP32 products and sums.
-    float const hxf = static_cast<float>(hx), hyf = static_cast<float>(hy),
-                hzf = static_cast<float>(hz);
+    // FP32 pre-test on positions in the group's frame: the staged records hold, rounded
+    // once to FP32, (w + shift - centre) h, with w the wrapped scaled coordinate, shift
+    // the period (-1, 0, 1) that places the record's window cell next to the group and
+    // centre the group's centre; every value is at most h/2 in size. Per coordinate the
+    // difference of two such values is off by at most 2^-24 h / 2 twice plus 2^-24 of
+    // itself; 1e-7 (h_x + h_y + h_z) and a 1e-6 relative widening of the radius cover
+    // that and the FP32 products and sums. Window offsets are the minimum image for every
+    // pair within the radius (6 or more half cells per edge), so no rint is needed.
+    double const ox = (2 * gx + 1.) / nx - 0.5, oy = (2 * gy + 1.) / ny - 0.5,
+                 oz = (2 * gz + 1.) / nz - 0.5;
     double const rpre = sqrt(rl2) * (1. + 1e-6) + 1e-7 * (hx + hy + hz);
     float const rpre2 = static_cast<float>(rpre * rpre * (1. + 1e-6));
+    // the same bound from inside: below rin2 in FP32 a pair is within the radius in exact
+    // arithmetic (and in the reference's FP64 test, whose rounding is far smaller), so only
+    // the candidates between rin2 and rpre2 need the FP64 test
+    double const rin = sqrt(rl2) * (1. - 1e-6) - 1e-7 * (hx + hy + hz);
+    float const rin2 = rin > 0. ? static_cast<float>(rin * rin * (1. - 1e-6)) : 0.f;
+    // half-cell widths
+    float const wxf = static_cast<float>(hx / nx), wyf = static_cast<float>(hy / ny),
+                wzf = static_cast<float>(hz / nz);
     int *queue = s_queue[warp];
-    unsigned const lt = (1u << lane) - 1u;
-    for (int c0 = 0; c0 < M; c0 += kStage) {
-        int const len = min(kStage, M - c0);
-        for (int t = threadIdx.x; t < len; t += blockDim.x) {
-            int const g = c0 + t;
-            int q = 0;
-            while (s_off[q + 1] <= g)
-                ++q;
-            int const j = A.cell_atoms[static_cast<size_t>(s_cell[q]) * cap + (g - s_off[q])];
-            s_j[t] = j;
+    for (int c0 = 0; c0 < M; c0 += kStageH) {
+        int const len = min(kStageH, M - c0);
+        __syncthreads(); // the previous chunk is done with
+        // one staged record per thread at a time: its window cell by bisection of the
+        // cells' offsets (the largest q with s_off[q] <= p, a non-empty cell)
+        for (int p = c0 + static_cast<int>(threadIdx.x); p < c0 + len;
+             p += static_cast<int>(blockDim.x)) {
+            int lo = 0, hi = kCells;
+            while (hi - lo > 1) {
+                int const mid = (lo + hi) >> 1;
+                if (s_off[mid] <= p)
+                    lo = mid;
+                else
+                    hi = mid;
+            }
+            int const q = lo;
+            int const u = q % kWin, v = (q / kWin) % kWin, w = q / (kWin * kWin);
+            int const ux = 2 * gx - 2 + u, uy = 2 * gy - 2 + v, uz = 2 * gz - 2 + w;
+            double const sx = (ux < 0 ? -1. : (ux >= nx ? 1. : 0.)) - ox,
+                         sy = (uy < 0 ? -1. : (uy >= ny ? 1. : 0.)) - oy,
+                         sz = (uz < 0 ? -1. : (uz >= nz ? 1. : 0.)) - oz;
+            int const j = A.cell_atoms[static_cast<size_t>(s_cell[q]) * cap + (p - s_off[q])];
             double4 const c = A.crd[j];
-            s_c[t] = c;
-            s_w[t] = make_float4(static_cast<float>(c.x - nint_ref(c.x)),
-                                 static_cast<float>(c.y - nint_ref(c.y)),
-                                 static_cast<float>(c.z - nint_ref(c.z)), 0.f);
+            s_j[p - c0] = j;
+            s_w[p - c0] = make_float4(static_cast<float>((c.x - nint_ref(c.x) + sx) * hx),
+                                      static_cast<float>((c.y - nint_ref(c.y) + sy) * hy),
+                                      static_cast<float>((c.z - nint_ref(c.z) + sz) * hz), 0.f);
         }
         __syncthreads();
         for (int a = warp; a < n_me; a += nwarp) {
-            int const i = me[a];
+            int const i = s_me[a], qa = s_mq[a];
+            int const ua = qa % kWin, va = (qa / kWin) % kWin, wa = qa / (kWin * kWin);
             double4 const ci = A.crd[i];
-            float const wx = static_cast<float>(ci.x - nint_ref(ci.x)),
-                        wy = static_cast<float>(ci.y - nint_ref(ci.y)),
-                        wz = static_cast<float>(ci.z - nint_ref(ci.z));
+            double const cwx = ci.x - nint_ref(ci.x), cwy = ci.y - nint_ref(ci.y),
+                         cwz = ci.z - nint_ref(ci.z);
+            // the atom in the group's frame (its own cell is never shifted)
+            float const wx = static_cast<float>((cwx - ox) * hx),
+                        wy = static_cast<float>((cwy - oy) * hy),
+                        wz = static_cast<float>((cwz - oz) * hz);
+            // the atom's fraction of its half cell along each edge
+            float const fx = fminf(fmaxf(static_cast<float>((cwx + 0.5) * nx - (2 * gx - 2 + ua)), 0.f), 1.f),
+                        fy = fminf(fmaxf(static_cast<float>((cwy + 0.5) * ny - (2 * gy - 2 + va)), 0.f), 1.f),
+                        fz = fminf(fmaxf(static_cast<float>((cwz + 0.5) * nz - (2 * gz - 2 + wa)), 0.f), 1.f);
             int nu = c_nu[a], nd = c_nd[a], total = c_tot[a];
             bool full = c_full[a] != 0;
             // exact test of the first n (<= 32) queued candidates, one per lane in order
+            // (queue entries: the staged index, with kNearEdge set when the FP32 distance
+            // lies between rin2 and rpre2)
             auto drain = [&](int n) {
-                int const k = static_cast<int>(lane) < n ? queue[lane] : -1;
+                int const qv = static_cast<int>(lane) < n ? queue[lane] : -1;
+                int const k = qv >= 0 ? (qv & ~kNearEdge) : -1;
                 int const j = k >= 0 ? s_j[k] : -1;
-                bool hit = false;
-                if (k >= 0) {
+                bool hit = k >= 0 && j != i; // the atom itself passes the pre-test
+                if (hit && (qv & kNearEdge)) {
                     double px, py, pz;
-                    hit = min_image_r2(ci, s_c[k], hx, hy, hz, px, py, pz) <= rl2;
+                    hit = min_image_r2(ci, A.crd[j], hx, hy, hz, px, py, pz) <= rl2;
                 }
                 nb_batch(A, i, j, hit, lane, nu, nd, total, full);
             };
-            int pend = 0;
-            for (int base = 0; base < len; base += 32) {
-                int const k = base + static_cast<int>(lane);
-                bool pass = false;
-                if (k < len && s_j[k] != i) {
-                    float4 const w = s_w[k];
-                    float dx = wx - w.x, dy = wy - w.y, dz = wz - w.z;
-                    dx = (dx - rintf(dx)) * hxf;
-                    dy = (dy - rintf(dy)) * hyf;
-                    dz = (dz - rintf(dz)) * hzf;
-                    pass = dx * dx + dy * dy + dz * dz <= rpre2;
+            // The atom's 25 rows of five half cells along x (fixed z, y offsets dw, dv), one
+            // per lane: rows whose lower distance bound exceeds the radius are dropped, the
+            // others trimmed along x to the cells within it (the bounds grow monotonically
+            // away from the atom's own column); each kept row is a run [s0, s1) of staged
+            // records, and the warp walks the non-empty runs in row order.
+            auto sq = [](float g, float w) { return (g * w) * (g * w); };
+            int rs0 = 0, rs1 = 0;
+            if (lane < 25) {
+                int const dw = static_cast<int>(lane) / 5 - 2, dv = static_cast<int>(lane) % 5 - 2;
+                float const ryz = sq(cell_gap(dw, fz), wzf) + sq(cell_gap(dv, fy), wyf);
+                if (ryz <= rpre2) {
+                    float const rem = rpre2 - ryz;
+                    int const ulo = -2 + (sq(cell_gap(-2, fx), wxf) > rem) +
+                                    (sq(cell_gap(-1, fx), wxf) > rem);
+                    int const uhi = 2 - (sq(cell_gap(2, fx), wxf) > rem) -
+                                    (sq(cell_gap(1, fx), wxf) > rem);
+                    int const row = ((wa + dw) * kWin + va + dv) * kWin + ua;
+                    rs0 = max(s_off[row + ulo], c0) - c0;
+                    rs1 = min(s_off[row + uhi + 1], c0 + len) - c0;
                 }
-                unsigned const bal = __ballot_sync(0xffffffffu, pass);
-                if (pass)
-                    queue[pend + __popc(bal & lt)] = k;
-                pend += __popc(bal);
-                __syncwarp();
-                if (pend >= 32) {
-                    drain(32);
+            }
+            unsigned rows = __ballot_sync(0xffffffffu, rs1 > rs0);
+            int pend = 0;
+            while (rows) {
+                int const rr = __ffs(rows) - 1;
+                rows &= rows - 1;
+                int const s0 = __shfl_sync(0xffffffffu, rs0, rr),
+                          s1 = __shfl_sync(0xffffffffu, rs1, rr);
+                for (int base = s0; base < s1; base += 32) {
+                    int const k = base + static_cast<int>(lane);
+                    bool pass = false, edge = false;
+                    if (k < s1) {
+                        float4 const w = s_w[k];
+                        float const dx = wx - w.x, dy = wy - w.y, dz = wz - w.z;
+                        float const r2 = dx * dx + dy * dy + dz * dz;
+                        pass = r2 <= rpre2;
+                        edge = !(r2 < rin2);
+                    }
+                    unsigned const bal = __ballot_sync(0xffffffffu, pass);
+                    if (pass)
+                        queue[pend + __popc(bal & lt)] = edge ? (k | kNearEdge) : k;
+                    pend += __popc(bal);
                     __syncwarp();
-                    if (static_cast<int>(lane) < pend - 32)
-                        queue[lane] = queue[32 + lane];
-                    pend -= 32;
-                    __syncwarp();
+                    if (pend >= 32) {
+                        drain(32);
+                        __syncwarp();
+                        if (static_cast<int>(lane) < pend - 32)
+                            queue[lane] = queue[32 + lane];
+                        pend -= 32;
+                        __syncwarp();
+                    }
                 }
             }
             if (pend > 0) {
@@ -260,32 +401,38 @@ __global__ void __launch_bounds__(128) k_nbr_cells(AtomsView A) {
                 c_full[a] = full ? 1 : 0;
             }
         }
-        __syncthreads();
     }
+    __syncthreads();
+    int tmax = 0;
     for (int a = threadIdx.x; a < n_me; a += blockDim.x) {
-        int const i = me[a];
+        int const i = s_me[a];
         A.n_up[i] = c_nu[a];
         A.n_dn[i] = c_nd[a];
         if (c_tot[a] > A.maxn) {
             status_or(&A.rep[r], MDELAST_ERR_LIST_OVERFLOW);
             set_halt(A);
         }
-        atomicMax(&A.max_count[0], c_tot[a]);
+        tmax = max(tmax, c_tot[a]);
     }
+    // the block's largest count, then one atomic per block (one per atom on a single
+    // address serialises in the L2)
+    tmax = __reduce_max_sync(0xffffffffu, tmax);
+    if (lane == 0)
+        atomicMax(&s_tmax, tmax);
+    __syncthreads();
+    if (threadIdx.x == 0)
+        atomicMax(&A.max_count[0], s_tmax);
 }
 
 size_t nbr_cells_smem(int cell_cap) {
-    return (sizeof(double4) + sizeof(float4) + sizeof(int)) * kStage +
-           4 * sizeof(int) * cell_cap;
+    return (sizeof(float4) + sizeof(int)) * kStageH + 8 * 6 * sizeof(int) * cell_cap;
 }
 
-// One warp per atom slot; the lanes test 32 candidates at a time. Atoms of cell-list
-// replicas are left to k_nbr_cells when cells_done, unless their cells are narrow.
-__global__ void k_nbr_build(AtomsView A, int cells_done) {
-    unsigned const lane = threadIdx.x & 31u;
-    int const i = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    if (i >= A.n_pad)
-        return;
+// One atom's list by one warp (all pairs, or the cells within the widened reach); the
+// lanes test 32 candidates at a time. Atoms of cell-list replicas are left to k_nbr_cells
+// when cells_done, unless their cells are narrow.
+__device__ __forceinline__ void nbr_build_atom(AtomsView const &A, int i, unsigned lane,
+                                               int cells_done) {
     int const r = A.rep_of[i];
     if (r < 0) {
         if (lane == 0) {
@@ -355,6 +502,21 @@ __global__ void k_nbr_build(AtomsView A, int cells_done) {
             set_halt(A);
         }
         atomicMax(&A.max_count[0], total);
+    }
+}
+
+// Grid-striding warps over the atoms of the replicas k_nbr_cells left (all when
+// !cells_done); the padding slots keep the zero counts of their allocation.
+__global__ void k_nbr_build(AtomsView A, int cells_done) {
+    unsigned const lane = threadIdx.x & 31u;
+    int const w0 = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    int const n_warps = static_cast<int>((gridDim.x * blockDim.x) >> 5);
+    for (int r = 0; r < A.n_rep; ++r) {
+        Replica const &R = A.rep[r];
+        if (cells_done && R.nc[0] != 0 && !narrow_cells(R, A.r_list_sq))
+            continue;
+        for (int a = w0; a < R.n_atoms; a += n_warps)
+            nbr_build_atom(A, R.atom_begin + a, lane, cells_done);
     }
 }
 
@@ -824,8 +986,22 @@ __device__ __forceinline__ void sublist_row(AtomsView const &A, int i, int lane,
             out[slot] = j;
     };
     unsigned const lt = (1u << lane) - 1u;
-    // shell of a squared distance: r / r_sub in units of kSubShell
+    // Mixed precision: the keep test runs in FP32 on the wrapped positions the pair passes
+    // read, with the minimum image they use (the same on both atoms of a pair, so the list
+    // stays symmetric), against the radius widened by 1e-5: every pair within it in exact
+    // arithmetic is kept, a few just beyond it too, which add zeros. FP64: the reference's
+    // min image and the exact radius.
+    bool const f32 = A.posf != nullptr;
+    float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
+    float3 L = make_float3(0.f, 0.f, 0.f), iL = L;
+    if (f32) {
+        pi = A.posf[i];
+        box_f(R, L, iL);
+    }
+    float const sub_r2f = static_cast<float>(A.sub_r2 / (kAng * kAng) * (1. + 1e-5));
+    // shell of a distance: r / r_sub in units of kSubShell (r in cm, or in A for FP32)
     float const inv_shell = 1.f / (kSubShell * static_cast<float>(sqrt(A.sub_r2)));
+    float const inv_shell_a = 1.f / (kSubShell * static_cast<float>(sqrt(A.sub_r2) / kAng));
     if (sorted) {
         s_cnt[lane] = 0;
         s_cnt[kSubShells + lane] = 0;
@@ -836,12 +1012,20 @@ __device__ __forceinline__ void sublist_row(AtomsView const &A, int i, int lane,
         int const k = k0 + lane;
         bool keep = false, upper = k < nu;
         int j = -1;
-        double r2 = 0.;
+        float rs = 0.f; // r in shell units
         if (k < nu + nd) {
             j = row[upper ? k : A.maxn - 1 - (k - nu)];
-            double px, py, pz;
-            r2 = min_image_r2(ci, A.crd[j], hx, hy, hz, px, py, pz);
-            keep = r2 <= A.sub_r2;
+            if (f32) {
+                float dx, dy, dz;
+                float const r2 = min_image_f(pi, A.posf[j], L, iL, dx, dy, dz);
+                keep = r2 <= sub_r2f;
+                rs = sqrtf(r2) * inv_shell_a;
+            } else {
+                double px, py, pz;
+                double const r2 = min_image_r2(ci, A.crd[j], hx, hy, hz, px, py, pz);
+                keep = r2 <= A.sub_r2;
+                rs = sqrtf(static_cast<float>(r2)) * inv_shell;
+            }
         }
         unsigned const bu = __ballot_sync(0xffffffffu, keep && upper);
         unsigned const bd = __ballot_sync(0xffffffffu, keep && !upper);
@@ -850,8 +1034,7 @@ __device__ __forceinline__ void sublist_row(AtomsView const &A, int i, int lane,
             // the back) with their shell in the top bits; shells counted per half
             if (keep) {
                 int const q = upper ? ku + __popc(bu & lt) : A.maxn - 1 - (kd + __popc(bd & lt));
-                int const sh = min(kSubShells - 1,
-                                   static_cast<int>(sqrtf(static_cast<float>(r2)) * inv_shell));
+                int const sh = min(kSubShells - 1, static_cast<int>(rs));
                 s_j[q] = (sh << 26) | (j - base);
                 atomicAdd(&s_cnt[(upper ? 0 : kSubShells) + sh], 1);
             }
@@ -916,7 +1099,8 @@ __host__ __device__ size_t sublist_smem(int maxn) {
     return b <= kSublistSortMax ? b : 0;
 }
 
-__global__ void __launch_bounds__(256) k_sublist(AtomsView A) {
+// 5 blocks of 256 threads per SM (the launch is 5 blocks per SM): at most 48 registers
+__global__ void __launch_bounds__(256, 5) k_sublist(AtomsView A) {
     if (halted(A)) // a list build ran out of capacity: nothing until the host regrows
         return;
     extern __shared__ int s_sub[];

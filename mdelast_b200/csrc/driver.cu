@@ -686,15 +686,15 @@ void mdelast_driver_s::drop_graphs() {
         }
 }
 
-// Cells per edge for the current box: no cell thinner than the list radius (with a margin
-// for the box changes of an NPT run between rebuilds); fewer than 3 along any edge means
-// an all-pairs search.
+// Half cells per edge for the current box: twice the number of cells no thinner than the
+// list radius (with a margin for the box changes of an NPT run between rebuilds); fewer
+// than 3 such cells along any edge means an all-pairs search.
 int mdelast_driver_s::configure_cells(std::vector<double> const &boxes) {
     // per replica: cells per edge from its box, and its block of the global cell arrays
     std::vector<Replica> R(static_cast<size_t>(n_rep));
     CK(cudaMemcpy(R.data(), d_rep, sizeof(Replica) * n_rep, cudaMemcpyDeviceToHost));
     bool changed = false, all_brute = true;
-    int n_cells = 0, cap = std::max(A.cell_cap, 64);
+    int n_cells = 0, cap = std::max(A.cell_cap, 32);
     for (int q = 0; q < n_rep; ++q) {
         int nc[3];
         bool brute = false;
@@ -702,6 +702,7 @@ int mdelast_driver_s::configure_cells(std::vector<double> const &boxes) {
             nc[a] = static_cast<int>(std::floor(boxes[3 * q + a] / (r_list * 1.05)));
             if (nc[a] < 3)
                 brute = true;
+            nc[a] *= 2;
         }
         if (brute)
             nc[0] = nc[1] = nc[2] = 0;
@@ -714,7 +715,7 @@ int mdelast_driver_s::configure_cells(std::vector<double> const &boxes) {
         r.cell_begin = n_cells;
         int const nq = brute ? 0 : nc[0] * nc[1] * nc[2];
         if (nq > 0)
-            cap = std::max(cap, static_cast<int>(2. * r.n_atoms / nq) + 64);
+            cap = std::max(cap, static_cast<int>(2. * r.n_atoms / nq) + 16);
         n_cells += nq;
         all_brute = all_brute && brute;
     }
@@ -756,19 +757,24 @@ int mdelast_driver_s::enqueue_rebuild() {
     if (!all_pairs && A.n_cells > 0) {
         CK(cudaMemsetAsync(d_cell_count, 0, sizeof(int) * A.n_cells, stream));
         k_cell_bin<<<grid, kBlock, 0, stream>>>(A);
-        k_cell_sort<<<A.n_cells, 128, sizeof(int) * A.cell_cap, stream>>>(A);
+        size_t const sort_smem = sizeof(int) * kCellSortWarps * A.cell_cap;
+        if (sort_smem > 48 * 1024)
+            CK(cudaFuncSetAttribute(k_cell_sort, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(sort_smem)));
+        k_cell_sort<<<(A.n_cells + kCellSortWarps - 1) / kCellSortWarps, 32 * kCellSortWarps,
+                      sort_smem, stream>>>(A);
     }
     int cells_done = 0;
     if (!all_pairs && A.n_cells > 0) {
+        // the dynamic part alone may stay below 48 KB while static + dynamic exceed it
         size_t const smem = nbr_cells_smem(A.cell_cap);
-        if (smem > 48 * 1024)
-            CK(cudaFuncSetAttribute(k_nbr_cells, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(smem)));
-        k_nbr_cells<<<A.n_cells, 128, smem, stream>>>(A);
+        CK(cudaFuncSetAttribute(k_nbr_cells, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(smem)));
+        k_nbr_cells<<<A.n_cells / 8, kNbrCellsThreads, smem, stream>>>(A);
         cells_done = 1;
     }
     // all-pairs replicas and padding slots: one warp per atom slot
-    k_nbr_build<<<n_pad / 8, 256, 0, stream>>>(A, cells_done);
+    k_nbr_build<<<std::min(n_pad / 8, 148 * 8), 256, 0, stream>>>(A, cells_done);
     if (A.crd_ref)
         k_sub_invalidate<<<1, 128, 0, stream>>>(A);
     CK(cudaGetLastError());

@@ -89,24 +89,6 @@ __device__ __forceinline__ void tabf_eval(const float *p, float t, float inv_h, 
     }
 }
 
-// minimum image of pi - pj in a box of edges L (positions wrapped into [-L/2, L/2))
-__device__ __forceinline__ float min_image_f(float4 pi, float4 pj, float3 L, float3 iL,
-                                             float &dx, float &dy, float &dz) {
-    dx = __fsub_rn(pi.x, pj.x);
-    dy = __fsub_rn(pi.y, pj.y);
-    dz = __fsub_rn(pi.z, pj.z);
-    dx = __fmaf_rn(-L.x, rintf(__fmul_rn(dx, iL.x)), dx);
-    dy = __fmaf_rn(-L.y, rintf(__fmul_rn(dy, iL.y)), dy);
-    dz = __fmaf_rn(-L.z, rintf(__fmul_rn(dz, iL.z)), dz);
-    return __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
-}
-
-__device__ __forceinline__ void box_f(Replica const *R, float3 &L, float3 &iL) {
-    L = make_float3(static_cast<float>(R->h[0] / kAng), static_cast<float>(R->h[1] / kAng),
-                    static_cast<float>(R->h[2] / kAng));
-    iL = make_float3(1.f / L.x, 1.f / L.y, 1.f / L.z);
-}
-
 } // namespace
 
 // FP32 wrapped positions of every atom from the FP64 coordinates and the current box.

@@ -13,6 +13,24 @@ __device__ __forceinline__ void status_or(Replica *rep, unsigned bits) {
 __device__ __forceinline__ bool halted(AtomsView const &A) { return *A.halt != 0; }
 __device__ __forceinline__ void set_halt(AtomsView const &A) { *A.halt = 1; }
 
+// minimum image of pi - pj in a box of edges L (positions wrapped into [-L/2, L/2))
+__device__ __forceinline__ float min_image_f(float4 pi, float4 pj, float3 L, float3 iL,
+                                             float &dx, float &dy, float &dz) {
+    dx = __fsub_rn(pi.x, pj.x);
+    dy = __fsub_rn(pi.y, pj.y);
+    dz = __fsub_rn(pi.z, pj.z);
+    dx = __fmaf_rn(-L.x, rintf(__fmul_rn(dx, iL.x)), dx);
+    dy = __fmaf_rn(-L.y, rintf(__fmul_rn(dy, iL.y)), dy);
+    dz = __fmaf_rn(-L.z, rintf(__fmul_rn(dz, iL.z)), dz);
+    return __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+}
+
+__device__ __forceinline__ void box_f(Replica const *R, float3 &L, float3 &iL) {
+    L = make_float3(static_cast<float>(R->h[0] / kAng), static_cast<float>(R->h[1] / kAng),
+                    static_cast<float>(R->h[2] / kAng));
+    iL = make_float3(1.f / L.x, 1.f / L.y, 1.f / L.z);
+}
+
 // Block-wide sum of NS per-thread values into out[0..NS), warp shuffles then shared
 // memory; deterministic for a fixed block size (NB threads).
 template <int NS, int NB = kBlock>
