@@ -963,8 +963,21 @@ __global__ void __launch_bounds__(kBlock) k_kick_drift(AtomsView A, TablesView T
 constexpr int kSubShells = 32;
 constexpr float kSubShell = 0.035f; // shell width / r_list; 32 shells reach 1.12 r_list
 
+// Radius and shell constants of the refresh, formed once per thread: the FP32 keep radius
+// (A^2, widened by 1e-5) and the inverse shell widths for r in cm and in A.
+struct SubConst {
+    float r2f, inv_shell, inv_shell_a;
+};
+
+__device__ __forceinline__ SubConst sub_const(AtomsView const &A) {
+    double const rs = sqrt(A.sub_r2);
+    return SubConst{static_cast<float>(A.sub_r2 / (kAng * kAng) * (1. + 1e-5)),
+                    static_cast<float>(1. / (kSubShell * rs)),
+                    static_cast<float>(kAng / (kSubShell * rs))};
+}
+
 __device__ __forceinline__ void sublist_row(AtomsView const &A, int i, int lane, bool sorted,
-                                            int *s_j, int *s_cnt) {
+                                            int *s_j, int *s_cnt, SubConst const &sc) {
     int const r = A.rep_of[i];
     if (r < 0)
         return;
@@ -991,17 +1004,18 @@ __device__ __forceinline__ void sublist_row(AtomsView const &A, int i, int lane,
     // stays symmetric), against the radius widened by 1e-5: every pair within it in exact
     // arithmetic is kept, a few just beyond it too, which add zeros. FP64: the reference's
     // min image and the exact radius.
+    // (the box edges in A by a product, not the pair passes' quotient: the list needs the
+    // same image on both atoms of a pair, not the pair passes' last bit)
     bool const f32 = A.posf != nullptr;
     float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
     float3 L = make_float3(0.f, 0.f, 0.f), iL = L;
     if (f32) {
         pi = A.posf[i];
-        box_f(R, L, iL);
+        L = make_float3(static_cast<float>(hx * 1e8), static_cast<float>(hy * 1e8),
+                        static_cast<float>(hz * 1e8));
+        iL = make_float3(__frcp_rn(L.x), __frcp_rn(L.y), __frcp_rn(L.z));
     }
-    float const sub_r2f = static_cast<float>(A.sub_r2 / (kAng * kAng) * (1. + 1e-5));
-    // shell of a distance: r / r_sub in units of kSubShell (r in cm, or in A for FP32)
-    float const inv_shell = 1.f / (kSubShell * static_cast<float>(sqrt(A.sub_r2)));
-    float const inv_shell_a = 1.f / (kSubShell * static_cast<float>(sqrt(A.sub_r2) / kAng));
+    float const sub_r2f = sc.r2f, ish = f32 ? sc.inv_shell_a : sc.inv_shell;
     if (sorted) {
         s_cnt[lane] = 0;
         s_cnt[kSubShells + lane] = 0;
@@ -1012,19 +1026,18 @@ __device__ __forceinline__ void sublist_row(AtomsView const &A, int i, int lane,
         int const k = k0 + lane;
         bool keep = false, upper = k < nu;
         int j = -1;
-        float rs = 0.f; // r in shell units
+        float r2s = 0.f; // r^2 in the units of ish (A^2 or cm^2)
         if (k < nu + nd) {
             j = row[upper ? k : A.maxn - 1 - (k - nu)];
             if (f32) {
                 float dx, dy, dz;
-                float const r2 = min_image_f(pi, A.posf[j], L, iL, dx, dy, dz);
-                keep = r2 <= sub_r2f;
-                rs = sqrtf(r2) * inv_shell_a;
+                r2s = min_image_f(pi, A.posf[j], L, iL, dx, dy, dz);
+                keep = r2s <= sub_r2f;
             } else {
                 double px, py, pz;
                 double const r2 = min_image_r2(ci, A.crd[j], hx, hy, hz, px, py, pz);
                 keep = r2 <= A.sub_r2;
-                rs = sqrtf(static_cast<float>(r2)) * inv_shell;
+                r2s = static_cast<float>(r2);
             }
         }
         unsigned const bu = __ballot_sync(0xffffffffu, keep && upper);
@@ -1034,7 +1047,7 @@ __device__ __forceinline__ void sublist_row(AtomsView const &A, int i, int lane,
             // the back) with their shell in the top bits; shells counted per half
             if (keep) {
                 int const q = upper ? ku + __popc(bu & lt) : A.maxn - 1 - (kd + __popc(bd & lt));
-                int const sh = min(kSubShells - 1, static_cast<int>(rs));
+                int const sh = min(kSubShells - 1, static_cast<int>(sqrtf(r2s) * ish));
                 s_j[q] = (sh << 26) | (j - base);
                 atomicAdd(&s_cnt[(upper ? 0 : kSubShells) + sh], 1);
             }
@@ -1116,8 +1129,9 @@ __global__ void __launch_bounds__(256, 5) k_sublist(AtomsView A) {
     int *s_j = s_sub + static_cast<size_t>(warp) * (A.maxn + 2 * kSubShells);
     int *s_cnt = s_j + A.maxn;
     int const n_warps = gridDim.x * (blockDim.x >> 5);
+    SubConst const sc = sub_const(A);
     for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < A.n_pad; i += n_warps)
-        sublist_row(A, i, lane, sorted, s_j, s_cnt);
+        sublist_row(A, i, lane, sorted, s_j, s_cnt, sc);
 }
 
 __global__ void k_sub_invalidate(AtomsView A) {
