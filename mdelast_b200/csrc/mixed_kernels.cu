@@ -122,8 +122,12 @@ __device__ __forceinline__ void warp_accumulate(double v, double *slot) {
 // accumulators instead of being carried in registers through the pair loop: the loop then
 // runs with about half the registers, so twice the warps per SM hide the latency of the
 // partner gathers.
+//
+// Bounded to 8 blocks of 128 threads per SM (64 registers; the compiler's own choice is 72,
+// 7 blocks): a few bytes of spills, and the extra warps hide more of the gather latency
+// (0.194 -> 0.182 ms at 16 x 13,500 atoms; 9 and 10 blocks spilled more and ran slower).
 template <bool OBS, int TPA, int IP, typename IX>
-__global__ void __launch_bounds__(kBlock) k_density_mx(AtomsView A, TablesView T) {
+__global__ void __launch_bounds__(kBlock, 8) k_density_mx(AtomsView A, TablesView T) {
     if (halted(A)) // a list build ran out of capacity: nothing until the host regrows
         return;
     constexpr int kF = TabFmt<IP>::kF;
