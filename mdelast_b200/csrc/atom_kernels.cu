@@ -527,109 +527,126 @@ __global__ void k_nbr_build(AtomsView A, int cells_done) {
 // so those per-atom Born and Laplacian terms (md_driver.cpp:410-419) are formed here and
 // g, h are never stored.
 
+// The block's FP64 sums (embedding energy, the per-atom Born term F''_i g_i g_i^T and
+// Laplacian term) are folded warp by warp after each atom group into per-warp shared
+// accumulators, not carried in registers through the pair loop.
 template <bool OBS, int TPA, int IP, typename IX>
 __global__ void __launch_bounds__(kBlock) k_density(AtomsView A, TablesView T) {
     if (halted(A)) // a list build ran out of capacity: nothing until the host regrows
         return;
     constexpr int kF = TabFmt<IP>::kF;
+    __shared__ double sacc[kBlock / 32][D_NSUM];
+    int const warp = threadIdx.x >> 5;
+    for (int k = threadIdx.x; k < (kBlock / 32) * D_NSUM; k += kBlock)
+        (&sacc[0][0])[k] = 0.;
+    __syncthreads();
     int const r = A.dblk_rep[blockIdx.x];
     Replica const *R = A.rep + r;
     int const lb = blockIdx.x - R->dblk_begin, nb = R->dblk_n;
     int const apb = kBlock / TPA, sub = threadIdx.x % TPA;
     int const n_slots = R->n_blocks * kBlock;
     double const hx = R->h[0], hy = R->h[1], hz = R->h[2];
-    double acc[D_NSUM];
-#pragma unroll
-    for (int k = 0; k < D_NSUM; ++k)
-        acc[k] = 0.;
     for (int a0 = lb * apb; a0 < n_slots; a0 += nb * apb) {
-    int const a = a0 + static_cast<int>(threadIdx.x) / TPA;
-    int const i = R->atom_begin + a;
-    bool const valid = a < R->n_atoms && T.has_eam;
-    double rho = 0.;
-    double g[6] = {0, 0, 0, 0, 0, 0}, hv[3] = {0, 0, 0};
-    double4 ci = make_double4(0., 0., 0., 0.);
-    if (valid) {
-        ci = A.crd[i];
-        int const ti = static_cast<int>(ci.w);
-        int const nu = A.pn_up[i], ntot = nu + A.pn_dn[i];
-        PairRow<IX> const row = pair_row<IX>(A, i, R->atom_begin);
-        // the next partner's index and record are loaded one iteration ahead
-        double4 cn = A.crd[sub < ntot ? row.at(list_slot(sub, nu, A.pmaxn)) : i];
-        for (int kk = sub; kk < ntot; kk += TPA) {
-            double4 const cj = cn;
-            if (kk + TPA < ntot)
-                cn = A.crd[row.at(list_slot(kk + TPA, nu, A.pmaxn))];
-            double px, py, pz;
-            double const r2 = min_image_r2(ci, cj, hx, hy, hz, px, py, pz);
-            if (r2 > T.r_cut_sq)
-                continue;
-            double const dr = sqrt(r2);
-            int const tj = static_cast<int>(cj.w);
-            if (dr > T.eam_rcut[tj])
-                continue;
-            double t;
-            int const k = tab_locate(dr, T.inv_hr, T.nri, t);
-            int const s = pair_slot(ti, tj);
-            int const off = (tj == (ti < tj ? ti : tj)) ? kF : 2 * kF;
-            double v = 0., d1 = 0., d2 = 0.;
-            tab_eval<IP, true, OBS, false>(T.rb + (static_cast<size_t>(s) * T.nri + k) * 3 * kF +
-                                               off,
-                                           t, T.inv_hr, T.inv_hr2, v, d1, d2);
-            rho += v;
-            if (OBS) {
-                double const ar = d1 / dr;
-                double const ap[3] = {ar * px, ar * py, ar * pz};
-                g[0] += ap[0] * px;
-                g[1] += ap[1] * py;
-                g[2] += ap[2] * pz;
-                g[3] += ap[1] * pz;
-                g[4] += ap[0] * pz;
-                g[5] += ap[0] * py;
-                hv[0] += ap[0];
-                hv[1] += ap[1];
-                hv[2] += ap[2];
+        int const a = a0 + static_cast<int>(threadIdx.x) / TPA;
+        int const i = R->atom_begin + a;
+        bool const valid = a < R->n_atoms && T.has_eam;
+        double rho = 0.;
+        double g[6] = {0, 0, 0, 0, 0, 0}, hv[3] = {0, 0, 0};
+        double4 ci = make_double4(0., 0., 0., 0.);
+        if (valid) {
+            ci = A.crd[i];
+            int const ti = static_cast<int>(ci.w);
+            int const nu = A.pn_up[i], ntot = nu + A.pn_dn[i];
+            PairRow<IX> const row = pair_row<IX>(A, i, R->atom_begin);
+            // the next partner's index and record are loaded one iteration ahead
+            double4 cn = A.crd[sub < ntot ? row.at(list_slot(sub, nu, A.pmaxn)) : i];
+            for (int kk = sub; kk < ntot; kk += TPA) {
+                double4 const cj = cn;
+                if (kk + TPA < ntot)
+                    cn = A.crd[row.at(list_slot(kk + TPA, nu, A.pmaxn))];
+                double px, py, pz;
+                double const r2 = min_image_r2(ci, cj, hx, hy, hz, px, py, pz);
+                if (r2 > T.r_cut_sq)
+                    continue;
+                double const dr = sqrt(r2);
+                int const tj = static_cast<int>(cj.w);
+                if (dr > T.eam_rcut[tj])
+                    continue;
+                double t;
+                int const k = tab_locate(dr, T.inv_hr, T.nri, t);
+                int const s = pair_slot(ti, tj);
+                int const off = (tj == (ti < tj ? ti : tj)) ? kF : 2 * kF;
+                double v = 0., d1 = 0., d2 = 0.;
+                tab_eval<IP, true, OBS, false>(
+                    T.rb + (static_cast<size_t>(s) * T.nri + k) * 3 * kF + off, t, T.inv_hr,
+                    T.inv_hr2, v, d1, d2);
+                rho += v;
+                if (OBS) {
+                    double const ar = d1 / dr;
+                    double const ap[3] = {ar * px, ar * py, ar * pz};
+                    g[0] += ap[0] * px;
+                    g[1] += ap[1] * py;
+                    g[2] += ap[2] * pz;
+                    g[3] += ap[1] * pz;
+                    g[4] += ap[0] * pz;
+                    g[5] += ap[0] * py;
+                    hv[0] += ap[0];
+                    hv[1] += ap[1];
+                    hv[2] += ap[2];
+                }
             }
         }
-    }
-    rho = group_sum<TPA>(rho);
-    if (OBS) {
-#pragma unroll
-        for (int a = 0; a < 6; ++a)
-            g[a] = group_sum<TPA>(g[a]);
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-            hv[a] = group_sum<TPA>(hv[a]);
-    }
-    if (valid && sub == 0) {
-        int const ti = static_cast<int>(ci.w);
-        // embedding function (eam.hpp:48-70); rho beyond rhomax_fatal ends the reference run
-        if (rho > T.rhomax[ti])
-            status_or(A.rep + r, MDELAST_FATAL_RHO_MAX);
-        double t;
-        int const k = tab_locate(rho, T.inv_hf, T.nfi, t);
-        double F = 0., dF = 0., d2F = 0.;
-        tab_eval<IP, true, true, OBS>(T.Ft + (static_cast<size_t>(ti) * T.nfi + k) * kF, t,
-                                      T.inv_hf, T.inv_hf2, F, dF, d2F);
-        A.rho[i] = rho;
-        A.Fe[i] = F;
-        if (OBS)
-            A.dF2[i] = make_double2(dF, d2F);
-        else
-            A.dF2[i].x = dF;
-        acc[D_FSUM] += F;
+        rho = group_sum<TPA>(rho);
         if (OBS) {
+#pragma unroll
+            for (int u = 0; u < 6; ++u)
+                g[u] = group_sum<TPA>(g[u]);
+#pragma unroll
+            for (int u = 0; u < 3; ++u)
+                hv[u] = group_sum<TPA>(hv[u]);
+        }
+        double F = 0., d2F = 0.;
+        bool const own = valid && sub == 0;
+        if (own) {
+            int const ti = static_cast<int>(ci.w);
+            // embedding function (eam.hpp:48-70); rho beyond rhomax_fatal ends the reference run
+            if (rho > T.rhomax[ti])
+                status_or(A.rep + r, MDELAST_FATAL_RHO_MAX);
+            double t;
+            int const k = tab_locate(rho, T.inv_hf, T.nfi, t);
+            double dF = 0.;
+            tab_eval<IP, true, true, OBS>(T.Ft + (static_cast<size_t>(ti) * T.nfi + k) * kF, t,
+                                          T.inv_hf, T.inv_hf2, F, dF, d2F);
+            A.rho[i] = rho;
+            A.Fe[i] = F;
+            if (OBS)
+                A.dF2[i] = make_double2(dF, d2F);
+            else
+                A.dF2[i].x = dF;
+        }
+        warp_accumulate(F, &sacc[warp][D_FSUM]);
+        if (OBS) {
+            // zero for lanes without an atom
+            if (!own)
+                d2F = 0.;
             int q = D_CB;
 #pragma unroll
             for (int u = 0; u < 6; ++u)
 #pragma unroll
                 for (int v = u; v < 6; ++v)
-                    acc[q++] += d2F * g[u] * g[v];
-            acc[D_LAP] += d2F * (hv[0] * hv[0] + hv[1] * hv[1] + hv[2] * hv[2]);
+                    warp_accumulate(d2F * g[u] * g[v], &sacc[warp][q++]);
+            warp_accumulate(d2F * (hv[0] * hv[0] + hv[1] * hv[1] + hv[2] * hv[2]),
+                            &sacc[warp][D_LAP]);
         }
     }
+    __syncthreads();
+    for (int k = threadIdx.x; k < D_NSUM; k += blockDim.x) {
+        double s = 0.;
+#pragma unroll
+        for (int w = 0; w < kBlock / 32; ++w)
+            s += sacc[w][k];
+        A.pd[static_cast<size_t>(blockIdx.x) * D_NSUM + k] = s;
     }
-    block_sum_store<D_NSUM>(acc, A.pd + static_cast<size_t>(blockIdx.x) * D_NSUM);
 }
 
 // ------------------------------------------------------------------------------------

@@ -107,15 +107,6 @@ __global__ void k_posf(AtomsView A) {
                             static_cast<float>(c.w));
 }
 
-// Sum v over the warp (fixed order) and add it to this warp's shared accumulator.
-__device__ __forceinline__ void warp_accumulate(double v, double *slot) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1)
-        v += __shfl_down_sync(0xffffffffu, v, o);
-    if ((threadIdx.x & 31) == 0)
-        *slot += v;
-}
-
 // Density pass of md_driver.cpp:195-277 in mixed precision (see k_density for the roles).
 // The block's FP64 sums (embedding energy, the per-atom Born term F''_i g_i g_i^T and
 // Laplacian term) are folded warp by warp after each atom group into per-warp shared

@@ -31,6 +31,15 @@ __device__ __forceinline__ void box_f(Replica const *R, float3 &L, float3 &iL) {
     iL = make_float3(1.f / L.x, 1.f / L.y, 1.f / L.z);
 }
 
+// Sum v over the warp (fixed order) and add it to this warp's shared accumulator.
+__device__ __forceinline__ void warp_accumulate(double v, double *slot) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0)
+        *slot += v;
+}
+
 // Block-wide sum of NS per-thread values into out[0..NS), warp shuffles then shared
 // memory; deterministic for a fixed block size (NB threads).
 template <int NS, int NB = kBlock>
