@@ -78,12 +78,12 @@ __global__ void k_cell_bin(AtomsView A) {
 
 // Order each cell's members by slot index (rank sort in shared memory), so that the list
 // and everything summed over it are deterministic. One warp per half cell (about 8 atoms),
-// kCellSortWarps cells per block.
+// blockDim.x / 32 cells per block.
 __global__ void k_cell_sort(AtomsView A) {
     extern __shared__ int s_mem[];
     __shared__ int s_max; // the block's largest cell count: one global atomic per block
     int const lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int const cell = blockIdx.x * kCellSortWarps + warp;
+    int const cell = blockIdx.x * static_cast<int>(blockDim.x >> 5) + warp;
     if (threadIdx.x == 0)
         s_max = 0;
     __syncthreads();

@@ -163,6 +163,7 @@ char const *fatal_message(unsigned bits) {
 
 struct mdelast_driver_s {
     int device = 0;
+    int smem_optin = 48 * 1024; // largest dynamic shared memory a block may opt into
     cudaStream_t stream = nullptr;
     int N = 0, n_pad = 0, n_rep = 1, ntypes = 0, npot = 0, n_blocks = 0;
     int tpa_d = 1, tpa_f = 1; // lanes per atom of the density and force passes
@@ -757,23 +758,31 @@ int mdelast_driver_s::enqueue_rebuild() {
     if (!all_pairs && A.n_cells > 0) {
         CK(cudaMemsetAsync(d_cell_count, 0, sizeof(int) * A.n_cells, stream));
         k_cell_bin<<<grid, kBlock, 0, stream>>>(A);
-        size_t const sort_smem = sizeof(int) * kCellSortWarps * A.cell_cap;
+        // one warp per half cell, as many per block as their scratch (cell_cap ints each)
+        // fits; a capacity beyond one warp's share fails here rather than at the launch
+        size_t const per_warp = sizeof(int) * static_cast<size_t>(A.cell_cap);
+        int const wpb = static_cast<int>(
+            std::min<size_t>(kCellSortWarps, static_cast<size_t>(smem_optin - 64) / per_warp));
+        if (wpb < 1)
+            return fail(MDELAST_ERR_CAPACITY, "cell capacity %d exceeds the shared memory of "
+                        "the cell sort", A.cell_cap);
+        size_t const sort_smem = per_warp * wpb;
         if (sort_smem > 48 * 1024)
             CK(cudaFuncSetAttribute(k_cell_sort, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(sort_smem)));
-        k_cell_sort<<<(A.n_cells + kCellSortWarps - 1) / kCellSortWarps, 32 * kCellSortWarps,
-                      sort_smem, stream>>>(A);
+        k_cell_sort<<<(A.n_cells + wpb - 1) / wpb, 32 * wpb, sort_smem, stream>>>(A);
     }
     int cells_done = 0;
-    if (!all_pairs && A.n_cells > 0) {
+    size_t const smem = nbr_cells_smem(A.cell_cap);
+    // cells so crowded that a group's staging does not fit: k_nbr_build walks the cells
+    if (!all_pairs && A.n_cells > 0 && smem + kNbrCellsStaticSmem <= static_cast<size_t>(smem_optin)) {
         // the dynamic part alone may stay below 48 KB while static + dynamic exceed it
-        size_t const smem = nbr_cells_smem(A.cell_cap);
         CK(cudaFuncSetAttribute(k_nbr_cells, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(smem)));
         k_nbr_cells<<<A.n_cells / 8, kNbrCellsThreads, smem, stream>>>(A);
         cells_done = 1;
     }
-    // all-pairs replicas and padding slots: one warp per atom slot
+    // all-pairs replicas, and cell replicas k_nbr_cells left (narrow or too crowded cells)
     k_nbr_build<<<std::min(n_pad / 8, 148 * 8), 256, 0, stream>>>(A, cells_done);
     if (A.crd_ref)
         k_sub_invalidate<<<1, 128, 0, stream>>>(A);
@@ -1138,6 +1147,9 @@ static int create_system(const mdelast_driver_config *cfgs, int n_rep, mdelast_d
 
     auto *d = new mdelast_driver_s();
     d->device = c0.device;
+    if (cudaDeviceGetAttribute(&d->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin,
+                               d->device) != cudaSuccess)
+        d->smem_optin = 48 * 1024;
     auto bail = [&](int rc) {
         delete d;
         return rc;

@@ -15,6 +15,7 @@ __global__ void k_nbr_cells(AtomsView A);
 size_t nbr_cells_smem(int cell_cap); // dynamic shared memory of k_nbr_cells
 constexpr int kCellSortWarps = 8;      // half cells per k_cell_sort block (one warp each)
 constexpr int kNbrCellsThreads = 256;   // threads of a k_nbr_cells block (one 2x2x2 half-cell group)
+constexpr size_t kNbrCellsStaticSmem = 4 * 1024; // bound on k_nbr_cells' static shared memory
 // launchers of the templated pair kernels (defined beside them); tpa = lanes per atom,
 // one of 1, 4, 8, 16 (valid_tpa)
 bool valid_tpa(int tpa);
