@@ -164,6 +164,9 @@ char const *fatal_message(unsigned bits) {
 struct mdelast_driver_s {
     int device = 0;
     int smem_optin = 48 * 1024; // largest dynamic shared memory a block may opt into
+    // k_nbr_cells for cell-list replicas (MDELAST_CELL_STAGING=0: k_nbr_build's per-atom
+    // cell walk for all, which gives the same list)
+    bool cell_staging = true;
     cudaStream_t stream = nullptr;
     int N = 0, n_pad = 0, n_rep = 1, ntypes = 0, npot = 0, n_blocks = 0;
     int tpa_d = 1, tpa_f = 1; // lanes per atom of the density and force passes
@@ -775,7 +778,8 @@ int mdelast_driver_s::enqueue_rebuild() {
     int cells_done = 0;
     size_t const smem = nbr_cells_smem(A.cell_cap);
     // cells so crowded that a group's staging does not fit: k_nbr_build walks the cells
-    if (!all_pairs && A.n_cells > 0 && smem + kNbrCellsStaticSmem <= static_cast<size_t>(smem_optin)) {
+    if (cell_staging && !all_pairs && A.n_cells > 0 &&
+        smem + kNbrCellsStaticSmem <= static_cast<size_t>(smem_optin)) {
         // the dynamic part alone may stay below 48 KB while static + dynamic exceed it
         CK(cudaFuncSetAttribute(k_nbr_cells, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(smem)));
@@ -1150,6 +1154,8 @@ static int create_system(const mdelast_driver_config *cfgs, int n_rep, mdelast_d
     if (cudaDeviceGetAttribute(&d->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin,
                                d->device) != cudaSuccess)
         d->smem_optin = 48 * 1024;
+    if (char const *e = std::getenv("MDELAST_CELL_STAGING"))
+        d->cell_staging = std::atoi(e) != 0;
     auto bail = [&](int rc) {
         delete d;
         return rc;
