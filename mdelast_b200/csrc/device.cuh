@@ -112,7 +112,10 @@ struct TablesView {
     // (type a at (npot + a) * st_n), 6 floats each, de-duplicated (each rho once, not once
     // per type pair). st_n == 0: no staged copy. st_bytes: its size (a multiple of 16).
     const float *stf;
-    int st_lo, st_n, st_bytes, st_pad;
+    int st_lo, st_n, st_bytes;
+    // fuc: every function's FP32 cutoff is at least the pair cutoff, so no per-function
+    // cutoff applies to a pair within it; the mixed passes then skip those tests
+    int fuc;
     float fpot_rcut[kMaxTypes * (kMaxTypes + 1) / 2];
     float fpot_rmin[kMaxTypes * (kMaxTypes + 1) / 2];
     float feam_rcut[kMaxTypes];

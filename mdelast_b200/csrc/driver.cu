@@ -1328,6 +1328,13 @@ static int create_system(const mdelast_driver_config *cfgs, int n_rep, mdelast_d
         }
         for (int t = 0; t < nt; ++t)
             T.feam_rcut[t] = static_cast<float>(T.eam_rcut[t] / kAng);
+        float const rcf = static_cast<float>(rcut / kAng);
+        T.fuc = 1;
+        for (int s = 0; s < npot; ++s)
+            T.fuc &= T.fpot_rcut[s] >= rcf;
+        if (T.has_eam)
+            for (int t = 0; t < nt; ++t)
+                T.fuc &= T.feam_rcut[t] >= rcf;
     }
 
     // ---- g(r) bins of each replica (md_driver.cpp:41): drg = rg[1] - rg[0],

@@ -107,6 +107,52 @@ __global__ void k_posf(AtomsView A) {
                             static_cast<float>(c.w));
 }
 
+// One lane's share of an atom row in the density pass: branch-free body, two entries per
+// unrolled pass, as in the force pass; an entry beyond the cutoff adds zeros. UC: every
+// density cutoff is at least the pair cutoff (no per-type test).
+template <bool OBS, int TPA, int IP, typename IX, bool UC>
+__device__ __forceinline__ void dens_loop(AtomsView const &A, TablesView const &T, float4 pi,
+                                          float3 L, float3 iL, PairRow<IX> const &row, int nu,
+                                          int ntot, int sub, double &rho, float (&g)[6],
+                                          float (&hv)[3]) {
+    float4 pn = A.posf[sub < ntot ? row.at(list_slot(sub, nu, A.pmaxn)) : row.base];
+#pragma unroll 2
+    for (int kk = sub; kk < ntot; kk += TPA) {
+        float4 const pj = pn;
+        pn = A.posf[row.at(list_slot(min(kk + TPA, ntot - 1), nu, A.pmaxn))];
+        float dx, dy, dz;
+        float const r2 = min_image_f(pi, pj, L, iL, dx, dy, dz);
+        float const idr = rsqrtf(r2);
+        float const dr = __fmul_rn(r2, idr);
+        int const tj = static_cast<int>(pj.w);
+        bool const in_cut = !(r2 > T.fr_cut_sq) && (UC || !(dr > T.feam_rcut[tj]));
+        float t;
+        int const k = tab_locate_f(dr, T.finv_hr, T.nri, t);
+        float v = 0.f, d1 = 0.f, d2 = 0.f;
+        tabf_eval<IP, true, OBS, false>(
+            T.rrf + (static_cast<size_t>(tj) * T.nri + k) * TabFmt<IP>::kFf, t, T.finv_hr,
+            T.finv_hr2, v, d1, d2);
+        if (!in_cut) {
+            v = 0.f;
+            d1 = 0.f;
+        }
+        rho += static_cast<double>(v);
+        if (OBS) {
+            float const ar = d1 * idr;
+            float const ap[3] = {ar * dx, ar * dy, ar * dz};
+            g[0] += ap[0] * dx;
+            g[1] += ap[1] * dy;
+            g[2] += ap[2] * dz;
+            g[3] += ap[1] * dz;
+            g[4] += ap[0] * dz;
+            g[5] += ap[0] * dy;
+            hv[0] += ap[0];
+            hv[1] += ap[1];
+            hv[2] += ap[2];
+        }
+    }
+}
+
 // Density pass of md_driver.cpp:195-277 in mixed precision (see k_density for the roles).
 // The block's FP64 sums (embedding energy, the per-atom Born term F''_i g_i g_i^T and
 // Laplacian term) are folded warp by warp after each atom group into per-warp shared
@@ -147,44 +193,12 @@ __global__ void __launch_bounds__(kBlock, 8) k_density_mx(AtomsView A, TablesVie
             ti = static_cast<int>(pi.w);
             int const nu = A.pn_up[i], ntot = nu + A.pn_dn[i];
             PairRow<IX> const row = pair_row<IX>(A, i, R->atom_begin);
-            float4 pn = A.posf[sub < ntot ? row.at(list_slot(sub, nu, A.pmaxn)) : i];
-            // branch-free body, two entries per unrolled pass, as in the force pass: an
-            // entry beyond the cutoff adds zeros
-#pragma unroll 2
-            for (int kk = sub; kk < ntot; kk += TPA) {
-                float4 const pj = pn;
-                pn = A.posf[row.at(list_slot(min(kk + TPA, ntot - 1), nu, A.pmaxn))];
-                float dx, dy, dz;
-                float const r2 = min_image_f(pi, pj, L, iL, dx, dy, dz);
-                float const idr = rsqrtf(r2);
-                float const dr = __fmul_rn(r2, idr);
-                int const tj = static_cast<int>(pj.w);
-                bool const in_cut = !(r2 > T.fr_cut_sq) && !(dr > T.feam_rcut[tj]);
-                float t;
-                int const k = tab_locate_f(dr, T.finv_hr, T.nri, t);
-                float v = 0.f, d1 = 0.f, d2 = 0.f;
-                tabf_eval<IP, true, OBS, false>(
-                    T.rrf + (static_cast<size_t>(tj) * T.nri + k) * TabFmt<IP>::kFf, t,
-                    T.finv_hr, T.finv_hr2, v, d1, d2);
-                if (!in_cut) {
-                    v = 0.f;
-                    d1 = 0.f;
-                }
-                rho += static_cast<double>(v);
-                if (OBS) {
-                    float const ar = d1 * idr;
-                    float const ap[3] = {ar * dx, ar * dy, ar * dz};
-                    g[0] += ap[0] * dx;
-                    g[1] += ap[1] * dy;
-                    g[2] += ap[2] * dz;
-                    g[3] += ap[1] * dz;
-                    g[4] += ap[0] * dz;
-                    g[5] += ap[0] * dy;
-                    hv[0] += ap[0];
-                    hv[1] += ap[1];
-                    hv[2] += ap[2];
-                }
-            }
+            // uniform cutoffs (every setfl potential): no per-function cutoff test
+            if (T.fuc)
+                dens_loop<OBS, TPA, IP, IX, true>(A, T, pi, L, iL, row, nu, ntot, sub, rho, g, hv);
+            else
+                dens_loop<OBS, TPA, IP, IX, false>(A, T, pi, L, iL, row, nu, ntot, sub, rho, g,
+                                                   hv);
         }
         rho = group_sum<TPA>(rho);
         if (OBS) {
@@ -312,7 +326,7 @@ __device__ __forceinline__ void pair_coefs(TablesView const &T, const float *sta
 // UPPER, else of partners j < i, addressed from the end of the row); every pair adds its
 // force and half its energy to the atom, and pairs j > i also add to the global sums.
 // STAGED: quintic tables read from the staged shared-memory copy `stab` where staged.
-template <bool OBS, bool UPPER, int TPA, int IP, bool STAGED, typename IX>
+template <bool OBS, bool UPPER, int TPA, int IP, bool STAGED, typename IX, bool UC>
 __device__ __forceinline__ void force_row_mx(AtomsView const &A, TablesView const &T,
                                              RowIn const &in, PairRow<IX> const &row, int n,
                                              int sub,
@@ -355,13 +369,13 @@ __device__ __forceinline__ void force_row_mx(AtomsView const &A, TablesView cons
         float drho_i = 0.f, drho_j = 0.f, d2rho_i = 0.f, d2rho_j = 0.f;
         if (in_cut && dr < T.fpot_rmin[s])
             warn_rmin = true;
-        bool const eam_i = T.has_eam && !(dr > T.feam_rcut[ti]);
-        bool const eam_j = T.has_eam && !(dr > T.feam_rcut[tj]);
+        bool const eam_i = T.has_eam && (UC || !(dr > T.feam_rcut[ti]));
+        bool const eam_j = T.has_eam && (UC || !(dr > T.feam_rcut[tj]));
         if constexpr (IP == MDELAST_QUINTIC) {
             // the three functions' coefficients first (independent loads), then the math
             float cp[6], ci[6], cj[6];
             pair_coefs<STAGED>(T, stab, s, ti, tj, k, cp, ci, cj);
-            if (!(dr > T.fpot_rcut[s])) {
+            if (UC || !(dr > T.fpot_rcut[s])) {
                 V = tabf_v(cp, t);
                 dV = tabf_d1(cp, t, T.finv_hr);
                 if (OBS)
@@ -379,7 +393,7 @@ __device__ __forceinline__ void force_row_mx(AtomsView const &A, TablesView cons
             }
         } else {
             const float *bundle = T.rbf + (static_cast<size_t>(s) * T.nri + k) * TabFmt<IP>::kB;
-            if (!(dr > T.fpot_rcut[s]))
+            if (UC || !(dr > T.fpot_rcut[s]))
                 tabf_eval<IP, true, true, OBS>(bundle, t, T.finv_hr, T.finv_hr2, V, dV, d2V);
             // rho'_{t_i} and rho'_{t_j} at r: rho_a of the bundle belongs to the smaller type
             int const oi = (ti <= tj) ? kFb : 2 * kFb, oj = (ti < tj) ? 2 * kFb : kFb;
@@ -517,10 +531,18 @@ __global__ void __launch_bounds__(NB) k_force_mx(AtomsView A, TablesView T) {
             PairRow<IX> const row = pair_row<IX>(A, i, R->atom_begin);
             bool warn_rmin = false;
             PairSums<OBS> ps;
-            force_row_mx<OBS, true, TPA, IP, STAGED, IX>(A, T, in, row, nu, sub, fx, fy, fz,
-                                                         epot, ps, warn_rmin, stab);
-            force_row_mx<OBS, false, TPA, IP, STAGED, IX>(A, T, in, row, nd, sub, fx, fy, fz,
-                                                          epot, ps, warn_rmin, stab);
+            // uniform cutoffs (every setfl potential): no per-function cutoff tests
+            if (T.fuc) {
+                force_row_mx<OBS, true, TPA, IP, STAGED, IX, true>(
+                    A, T, in, row, nu, sub, fx, fy, fz, epot, ps, warn_rmin, stab);
+                force_row_mx<OBS, false, TPA, IP, STAGED, IX, true>(
+                    A, T, in, row, nd, sub, fx, fy, fz, epot, ps, warn_rmin, stab);
+            } else {
+                force_row_mx<OBS, true, TPA, IP, STAGED, IX, false>(
+                    A, T, in, row, nu, sub, fx, fy, fz, epot, ps, warn_rmin, stab);
+                force_row_mx<OBS, false, TPA, IP, STAGED, IX, false>(
+                    A, T, in, row, nd, sub, fx, fy, fz, epot, ps, warn_rmin, stab);
+            }
             if (warn_rmin)
                 status_or(A.rep + r, MDELAST_WARN_RMIN);
             sums[F_VIRIAL] = (ps.sig_d[0] + ps.sig_d[1]) + ps.sig_d[2];

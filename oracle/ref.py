@@ -128,7 +128,8 @@ class RefDriver:
         Tb, qb, p_eta_b, nf_b = baro_thermo
         self.h = L.create(
             t.n_types, interpolation.encode(), t.rcut, t.rmin_fatal, t.dr, t.n_r,
-            d(t.phi), d(t.dphi), d(t.d2phi), int(has_eam), t.rcut, t.rhomax, t.drho, t.n_rho,
+            d(t.phi), d(t.dphi), d(t.d2phi), int(has_eam), getattr(t, "eam_rcut", t.rcut),
+            t.rhomax, t.drho, t.n_rho,
             d(t.rho), d(t.drho_dr), d(t.d2rho_dr2), d(t.F), d(t.dF), d(t.d2F),
             N, d(positions), d(velocities), types.ctypes.data_as(U), d(t.masses),
             int(ensemble), int(coupling),
