@@ -546,6 +546,7 @@ __global__ void __launch_bounds__(kBlock) k_density(AtomsView A, TablesView T) {
     int const apb = kBlock / TPA, sub = threadIdx.x % TPA;
     int const n_slots = R->n_blocks * kBlock;
     double const hx = R->h[0], hy = R->h[1], hz = R->h[2];
+    bool const uc = T.uc64 != 0; // one cutoff for every function: no per-type test
     for (int a0 = lb * apb; a0 < n_slots; a0 += nb * apb) {
         int const a = a0 + static_cast<int>(threadIdx.x) / TPA;
         int const i = R->atom_begin + a;
@@ -570,7 +571,7 @@ __global__ void __launch_bounds__(kBlock) k_density(AtomsView A, TablesView T) {
                     continue;
                 double const dr = sqrt(r2);
                 int const tj = static_cast<int>(cj.w);
-                if (dr > T.eam_rcut[tj])
+                if (!uc && dr > T.eam_rcut[tj])
                     continue;
                 double t;
                 int const k = tab_locate(dr, T.inv_hr, T.nri, t);
@@ -678,7 +679,7 @@ struct RowIn64 {
     double hx, hy, hz;
 };
 
-template <bool OBS, bool UPPER, int TPA, int IP, typename IX>
+template <bool OBS, bool UPPER, int TPA, int IP, typename IX, bool UC>
 __device__ __forceinline__ void force_row(AtomsView const &A, TablesView const &T,
                                           RowIn64 const &in, PairRow<IX> const &row, int n,
                                           int sub, double &fx, double &fy, double &fz,
@@ -716,7 +717,7 @@ __device__ __forceinline__ void force_row(AtomsView const &A, TablesView const &
         double V = 0., dV = 0., d2V = 0.;
         if (dr < T.pot_rmin[s])
             warn_rmin = true;
-        if (!(dr > T.pot_rcut[s]))
+        if (UC || !(dr > T.pot_rcut[s]))
             tab_eval<IP, true, true, OBS && UPPER>(bundle, t, T.inv_hr, T.inv_hr2, V, dV, d2V);
         double dedr = dV;
         double X = 0., lap = 0.;
@@ -728,10 +729,10 @@ __device__ __forceinline__ void force_row(AtomsView const &A, TablesView const &
             // rho of the lower type at bundle offset kF, of the higher type at 2 kF
             int const oi = (ti <= tj) ? kF : 2 * kF, oj = (ti < tj) ? 2 * kF : kF;
             double drho_i = 0., drho_j = 0., d2rho_i = 0., d2rho_j = 0., unused = 0.;
-            if (!(dr > T.eam_rcut[ti]))
+            if (UC || !(dr > T.eam_rcut[ti]))
                 tab_eval<IP, false, true, OBS && UPPER>(bundle + oi, t, T.inv_hr, T.inv_hr2,
                                                         unused, drho_i, d2rho_i);
-            if (!(dr > T.eam_rcut[tj]))
+            if (UC || !(dr > T.eam_rcut[tj]))
                 tab_eval<IP, false, true, OBS && UPPER>(bundle + oj, t, T.inv_hr, T.inv_hr2,
                                                         unused, drho_j, d2rho_j);
             double const dFj = dFj2.x;
@@ -825,10 +826,18 @@ __global__ void __launch_bounds__(kBlock) k_force(AtomsView A, TablesView T) {
             PairRow<IX> const row = pair_row<IX>(A, i, R->atom_begin);
             bool warn_rmin = false;
             RowSums64<OBS> ps;
-            force_row<OBS, true, TPA, IP, IX>(A, T, in, row, nu, sub, fx, fy, fz, epot, ps,
-                                              warn_rmin);
-            force_row<OBS, false, TPA, IP, IX>(A, T, in, row, nd, sub, fx, fy, fz, epot, ps,
-                                               warn_rmin);
+            // one cutoff for every function (every setfl potential): no per-function tests
+            if (T.uc64) {
+                force_row<OBS, true, TPA, IP, IX, true>(A, T, in, row, nu, sub, fx, fy, fz,
+                                                        epot, ps, warn_rmin);
+                force_row<OBS, false, TPA, IP, IX, true>(A, T, in, row, nd, sub, fx, fy, fz,
+                                                         epot, ps, warn_rmin);
+            } else {
+                force_row<OBS, true, TPA, IP, IX, false>(A, T, in, row, nu, sub, fx, fy, fz,
+                                                         epot, ps, warn_rmin);
+                force_row<OBS, false, TPA, IP, IX, false>(A, T, in, row, nd, sub, fx, fy, fz,
+                                                          epot, ps, warn_rmin);
+            }
             if (warn_rmin)
                 status_or(A.rep + r, MDELAST_WARN_RMIN);
             sums[F_VIRIAL] = ps.virial;

@@ -114,8 +114,10 @@ struct TablesView {
     const float *stf;
     int st_lo, st_n, st_bytes;
     // fuc: every function's FP32 cutoff is at least the pair cutoff, so no per-function
-    // cutoff applies to a pair within it; the mixed passes then skip those tests
-    int fuc;
+    // cutoff applies to a pair within it; the mixed passes then skip those tests. uc64: the
+    // same in FP64, exactly: every cutoff is at least sqrt(r_cut_sq), the largest distance
+    // the FP64 passes compute for a pair with r^2 <= r_cut_sq (sqrt is correctly rounded)
+    int fuc, uc64;
     float fpot_rcut[kMaxTypes * (kMaxTypes + 1) / 2];
     float fpot_rmin[kMaxTypes * (kMaxTypes + 1) / 2];
     float feam_rcut[kMaxTypes];

@@ -1238,6 +1238,15 @@ static int create_system(const mdelast_driver_config *cfgs, int n_rep, mdelast_d
         T.rhomax[t] = c0.n_eam ? c0.eam[t]->rhomax_fatal : 0.;
         T.mass[t] = c0.mass[t];
     }
+    {
+        double const rc64 = std::sqrt(T.r_cut_sq);
+        T.uc64 = 1;
+        for (int s = 0; s < npot; ++s)
+            T.uc64 &= T.pot_rcut[s] >= rc64;
+        if (T.has_eam)
+            for (int t = 0; t < nt; ++t)
+                T.uc64 &= T.eam_rcut[t] >= rc64;
+    }
     d->precision = c0.precision;
     if (c0.precision == MDELAST_PRECISION_MIXED) {
         // The r tables in FP32, angstrom / eV (phi) and angstrom^-3 (rho): per type pair
