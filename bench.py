@@ -815,8 +815,8 @@ def half_list_nbar(m, t, cell):
 # replicas without cache flushing (the launches of timed-region steps, so the L2 holds
 # what the preceding kernels of the step left in it), mean over the captured launches;
 # profiles/launches_bench_mixed_16x13500.md has the capture. None where not captured.
-TRAFFIC_PER_LAUNCH: dict = {("mixed", 16, False): 82.59e6 + 1.10e6,
-                            ("mixed", 16, True): 79.19e6 + 0.80e6}
+TRAFFIC_PER_LAUNCH: dict = {("mixed", 16, False): 82.38e6 + 1.11e6,
+                            ("mixed", 16, True): 78.89e6 + 0.77e6}
 
 
 # ----------------------------------------------------------------------------- reference
