@@ -715,7 +715,7 @@ class BatchedMDDriver {
   public:
     BatchedMDDriver(std::vector<py::array_t<double, py::array::c_style | py::array::forcecast>> const &positions,
                     std::vector<py::array_t<double, py::array::c_style | py::array::forcecast>> const &velocities,
-                    std::vector<std::vector<unsigned>> const &types,
+                    std::vector<py::array_t<uint32_t, py::array::c_style | py::array::forcecast>> const &types,
                     std::vector<PotentialPtr> const &pot, std::vector<EAMPtr> const &eam,
                     std::vector<Ensamble> const &ensembles, std::vector<Thermostat> const &thermostats,
                     std::vector<Barostat> const &barostats, std::vector<Box> const &boxes,
@@ -739,7 +739,7 @@ class BatchedMDDriver {
         for (size_t r = 0; r < R; ++r) {
             auto const &P = positions[r];
             auto const &V = velocities[r];
-            size_t const N = types[r].size();
+            size_t const N = static_cast<size_t>(types[r].size());
             if (P.size() != static_cast<py::ssize_t>(3 * N) || V.size() != static_cast<py::ssize_t>(3 * N))
                 throw py::value_error("positions/velocities of a replica must be (N, 3)");
             mdelast_driver_config &c = cfg[r];
@@ -748,7 +748,7 @@ class BatchedMDDriver {
             c.n_types = static_cast<int32_t>(mass.size());
             c.positions = P.data();
             c.velocities = V.data();
-            c.types = reinterpret_cast<uint32_t const *>(types[r].data());
+            c.types = types[r].data();
             c.mass = mass_.data();
             c.pair = ph.data();
             c.eam = eh.data();
@@ -1098,7 +1098,8 @@ PYBIND11_MODULE(md_driver_module, m) {
     py::class_<BatchedMDDriver, std::shared_ptr<BatchedMDDriver>>(m, "BatchedMDDriver")
         .def(py::init<std::vector<py::array_t<double, py::array::c_style | py::array::forcecast>> const &,
                       std::vector<py::array_t<double, py::array::c_style | py::array::forcecast>> const &,
-                      std::vector<std::vector<unsigned>> const &, std::vector<PotentialPtr> const &,
+                      std::vector<py::array_t<uint32_t, py::array::c_style | py::array::forcecast>> const &,
+                      std::vector<PotentialPtr> const &,
                       std::vector<EAMPtr> const &, std::vector<Ensamble> const &,
                       std::vector<Thermostat> const &, std::vector<Barostat> const &,
                       std::vector<Box> const &, std::vector<double> const &,

@@ -174,7 +174,8 @@ def make_batch(m, tables: SetflTables, cells: list[Cell], dt=2e-15, neighbors=Tr
         rg = rg_bins(min(cells, key=lambda c: min(c.box)))
     ths, baros = zip(*[_thermostats(m, c) for c in cells])
     return m.BatchedMDDriver([c.positions for c in cells], [c.velocities for c in cells],
-                             [[int(t) for t in c.types] for c in cells], m.PotentialVector(pots),
+                             [np.asarray(c.types, dtype=np.uint32) for c in cells],
+                             m.PotentialVector(pots),
                              m.EAMVector(eams), [m.MDDriver.Ensamble(c.ensemble) for c in cells],
                              list(ths), list(baros), [m.Box(np.diag(c.box)) for c in cells],
                              [c.Nf for c in cells], list(tables.masses), dt,
