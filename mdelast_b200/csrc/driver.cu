@@ -83,6 +83,30 @@ template <typename T> void dfree(T *&p) {
     p = nullptr;
 }
 
+// Host staging of a creation's atom uploads: pinned, kept from one creation to the next (a
+// batch created after another reuses it instead of faulting in and pinning fresh pages),
+// used by one creation at a time under its mutex. mdelast_release_cached_memory() frees it.
+std::mutex g_stage_mutex;
+void *g_stage = nullptr;
+size_t g_stage_bytes = 0;
+
+// at least `bytes` of pinned staging (nullptr on failure); call with g_stage_mutex held
+void *stage_host(size_t bytes) {
+    if (bytes > g_stage_bytes) {
+        if (g_stage)
+            cudaFreeHost(g_stage);
+        g_stage = nullptr;
+        g_stage_bytes = 0;
+        if (cudaHostAlloc(&g_stage, bytes, cudaHostAllocPortable) != cudaSuccess) {
+            cudaGetLastError();
+            g_stage = nullptr;
+            return nullptr;
+        }
+        g_stage_bytes = bytes;
+    }
+    return g_stage;
+}
+
 double nint_host(double x) { // md_driver.hpp:48-50
     return static_cast<double>(x < 0. ? static_cast<int>(x - 0.5) : static_cast<int>(x + 0.5));
 }
@@ -990,6 +1014,13 @@ int mdelast_release_cached_memory(int32_t device) {
     }
     if (pool)
         CK(cudaMemPoolTrimTo(pool, 0));
+    {
+        std::lock_guard<std::mutex> lock(g_stage_mutex);
+        if (g_stage)
+            cudaFreeHost(g_stage);
+        g_stage = nullptr;
+        g_stage_bytes = 0;
+    }
     return MDELAST_OK;
 }
 
@@ -1113,11 +1144,6 @@ static int create_system(const mdelast_driver_config *cfgs, int n_rep, mdelast_d
         np += (cfgs[r].n_atoms + kTile - 1) / kTile * kTile;
         n_total += cfgs[r].n_atoms;
     }
-    std::vector<double4> crd(static_cast<size_t>(np), make_double4(0, 0, 0, 0));
-    std::vector<int> rep_of(static_cast<size_t>(np), -1);
-    std::vector<double> vel(3 * static_cast<size_t>(np), 0.);
-    std::vector<double> pos0(3 * static_cast<size_t>(n_total));
-    long p0off = 0;
     for (int r = 0; r < n_rep; ++r) {
         mdelast_driver_config const &c = cfgs[r];
         double const L[3] = {c.box[0], c.box[4], c.box[8]};
@@ -1128,6 +1154,36 @@ static int create_system(const mdelast_driver_config *cfgs, int n_rep, mdelast_d
                 return fail(MDELAST_ERR_ARGUMENT, "bad initial position (replica %d atom %d)", r, a);
             if (c.types[a] >= static_cast<uint32_t>(nt))
                 return fail(MDELAST_ERR_ARGUMENT, "bad type (replica %d atom %d)", r, a);
+        }
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(MDELAST_ERR_NO_DEVICE, "no CUDA device: the mdelast GPU path needs one");
+    }
+    if (c0.device < 0 || c0.device >= ndev)
+        return fail(MDELAST_ERR_ARGUMENT, "device %d not present (%d devices)", c0.device, ndev);
+    CK(cudaSetDevice(c0.device));
+    // scaled coordinates and type, velocities (SoA), replica of each slot, and the initial
+    // positions, written straight into the pinned staging that uploads them
+    std::unique_lock<std::mutex> stage_lock(g_stage_mutex);
+    size_t const b_crd = sizeof(double4) * static_cast<size_t>(np),
+                 b_vel = sizeof(double) * 3 * static_cast<size_t>(np),
+                 b_pos0 = sizeof(double) * 3 * static_cast<size_t>(n_total),
+                 b_rep = sizeof(int) * static_cast<size_t>(np);
+    char *stage = static_cast<char *>(stage_host(b_crd + b_vel + b_pos0 + b_rep));
+    if (!stage)
+        return fail(MDELAST_ERR_CUDA, "pinned host staging allocation failed");
+    double4 *crd = reinterpret_cast<double4 *>(stage);
+    double *vel = reinterpret_cast<double *>(stage + b_crd);
+    double *pos0 = reinterpret_cast<double *>(stage + b_crd + b_vel);
+    int *rep_of = reinterpret_cast<int *>(stage + b_crd + b_vel + b_pos0);
+    long p0off = 0;
+    for (int r = 0; r < n_rep; ++r) {
+        mdelast_driver_config const &c = cfgs[r];
+        double const L[3] = {c.box[0], c.box[4], c.box[8]};
+        for (int a = 0; a < c.n_atoms; ++a) {
+            double const *p = c.positions + 3 * a;
             double const u[3] = {p[0] / L[0], p[1] / L[1], p[2] / L[2]};
             size_t const i = static_cast<size_t>(begin[r] + a);
             crd[i] = make_double4(u[0] - nint_host(u[0]), u[1] - nint_host(u[1]),
@@ -1138,16 +1194,16 @@ static int create_system(const mdelast_driver_config *cfgs, int n_rep, mdelast_d
                 pos0[static_cast<size_t>(p0off + 3 * a + k)] = p[k];
             }
         }
+        // padding slots up to the next replica's block: no atom
+        int const end = r + 1 < n_rep ? begin[r + 1] : np;
+        for (int i = begin[r] + c.n_atoms; i < end; ++i) {
+            crd[i] = make_double4(0., 0., 0., 0.);
+            rep_of[i] = -1;
+            for (int k = 0; k < 3; ++k)
+                vel[static_cast<size_t>(k) * np + i] = 0.;
+        }
         p0off += 3L * c.n_atoms;
     }
-    int ndev = 0;
-    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
-        cudaGetLastError();
-        return fail(MDELAST_ERR_NO_DEVICE, "no CUDA device: the mdelast GPU path needs one");
-    }
-    if (c0.device < 0 || c0.device >= ndev)
-        return fail(MDELAST_ERR_ARGUMENT, "device %d not present (%d devices)", c0.device, ndev);
-    CK(cudaSetDevice(c0.device));
 
     auto *d = new mdelast_driver_s();
     d->device = c0.device;
@@ -1442,7 +1498,7 @@ static int create_system(const mdelast_driver_config *cfgs, int n_rep, mdelast_d
     d->cap_red = static_cast<size_t>(n_rep) * max_chunks * 64;
     TRY(dalloc(&d->d_max_count, 2));
     TRY(dalloc(&d->d_halt, 1));
-    TRY(dalloc(&d->d_pos0, pos0.size()));
+    TRY(dalloc(&d->d_pos0, 3 * static_cast<size_t>(n_total)));
     int max_n = 0;
     for (int r = 0; r < n_rep; ++r)
         max_n = std::max(max_n, count[r]);
@@ -1450,11 +1506,13 @@ static int create_system(const mdelast_driver_config *cfgs, int n_rep, mdelast_d
     d->pos0_off.assign(static_cast<size_t>(n_rep), 0);
     for (int r = 1; r < n_rep; ++r)
         d->pos0_off[r] = d->pos0_off[r - 1] + 3L * count[r - 1];
-    if (cudaMemcpy(d->d_rep_of, rep_of.data(), sizeof(int) * np, cudaMemcpyHostToDevice) ||
-        cudaMemcpy(d->d_crd, crd.data(), sizeof(double4) * np, cudaMemcpyHostToDevice) ||
-        cudaMemcpy(d->d_vel, vel.data(), sizeof(double) * vel.size(), cudaMemcpyHostToDevice) ||
-        cudaMemcpy(d->d_pos0, pos0.data(), sizeof(double) * pos0.size(), cudaMemcpyHostToDevice))
+    if (cudaMemcpyAsync(d->d_rep_of, rep_of, b_rep, cudaMemcpyHostToDevice, d->stream) ||
+        cudaMemcpyAsync(d->d_crd, crd, b_crd, cudaMemcpyHostToDevice, d->stream) ||
+        cudaMemcpyAsync(d->d_vel, vel, b_vel, cudaMemcpyHostToDevice, d->stream) ||
+        cudaMemcpyAsync(d->d_pos0, pos0, b_pos0, cudaMemcpyHostToDevice, d->stream) ||
+        cudaStreamSynchronize(d->stream))
         return bail(fail(MDELAST_ERR_CUDA, "atom upload failed"));
+    stage_lock.unlock(); // the staging is free for the next creation
     if (cudaMallocHost(&d->h_obs, sizeof(mdelast_observables) * n_rep) ||
         cudaEventCreateWithFlags(&d->ev_step, cudaEventDisableTiming))
         return bail(fail(MDELAST_ERR_CUDA, "host staging allocation failed"));
