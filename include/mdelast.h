@@ -68,8 +68,9 @@ int mdelast_abi_version(void);
 int mdelast_device_available(void);
 /* Drivers take their device buffers from a stream-ordered memory pool of the library's
  * own (one per device; the device's default pool is not touched), which keeps freed memory
- * for the next driver; this hands the unused part of it back to the device. No reference
- * counterpart (the reference holds host memory only). */
+ * for the next driver, and stage their atom uploads in a pinned host buffer kept for the
+ * next creation; this hands the unused part of the pool back to the device and frees the
+ * pinned buffer. No reference counterpart (the reference holds host memory only). */
 int mdelast_release_cached_memory(int32_t device);
 
 /* ---------------------------------------------------------------------------------
