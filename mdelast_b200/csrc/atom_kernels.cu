@@ -559,12 +559,15 @@ __global__ void __launch_bounds__(kBlock) k_density(AtomsView A, TablesView T) {
             int const ti = static_cast<int>(ci.w);
             int const nu = A.pn_up[i], ntot = nu + A.pn_dn[i];
             PairRow<IX> const row = pair_row<IX>(A, i, R->atom_begin);
-            // the next partner's index and record are loaded one iteration ahead
+            // the next partner's record is loaded one iteration ahead, its list entry two
             double4 cn = A.crd[sub < ntot ? row.at(list_slot(sub, nu, A.pmaxn)) : i];
+            int jn = sub < ntot ? row.at(list_slot(min(sub + TPA, ntot - 1), nu, A.pmaxn)) : i;
             for (int kk = sub; kk < ntot; kk += TPA) {
                 double4 const cj = cn;
-                if (kk + TPA < ntot)
-                    cn = A.crd[row.at(list_slot(kk + TPA, nu, A.pmaxn))];
+                if (kk + TPA < ntot) {
+                    cn = A.crd[jn];
+                    jn = row.at(list_slot(min(kk + 2 * TPA, ntot - 1), nu, A.pmaxn));
+                }
                 double px, py, pz;
                 double const r2 = min_image_r2(ci, cj, hx, hy, hz, px, py, pz);
                 if (r2 > T.r_cut_sq)
@@ -690,17 +693,18 @@ __device__ __forceinline__ void force_row(AtomsView const &A, TablesView const &
     auto slot = [&](int k) { return UPPER ? k : A.pmaxn - 1 - k; };
     int const ti = in.ti;
     double const dFi = in.dFi, d2Fi = in.d2Fi;
-    // the next partner's index, record and F' are loaded one iteration ahead
+    // the next partner's record and F' are loaded one iteration ahead, its list entry two
     int jn = row.at(slot(sub));
     double4 cn = A.crd[jn];
     double2 fn = A.dF2[jn];
+    jn = row.at(slot(min(sub + TPA, n - 1)));
     for (int kk = sub; kk < n; kk += TPA) {
         double4 const cj = cn;
         double2 const dFj2 = fn;
         if (kk + TPA < n) {
-            jn = row.at(slot(kk + TPA));
             cn = A.crd[jn];
             fn = A.dF2[jn];
+            jn = row.at(slot(min(kk + 2 * TPA, n - 1)));
         }
         double px, py, pz;
         double const r2 = min_image_r2(in.ci, cj, in.hx, in.hy, in.hz, px, py, pz);

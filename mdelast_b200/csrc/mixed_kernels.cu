@@ -115,11 +115,15 @@ __device__ __forceinline__ void dens_loop(AtomsView const &A, TablesView const &
                                           float3 L, float3 iL, PairRow<IX> const &row, int nu,
                                           int ntot, int sub, double &rho, float (&g)[6],
                                           float (&hv)[3]) {
+    // the next partner's record and the list entry after it are loaded ahead, so the
+    // entry's load does not delay the record's
     float4 pn = A.posf[sub < ntot ? row.at(list_slot(sub, nu, A.pmaxn)) : row.base];
+    int jn = sub < ntot ? row.at(list_slot(min(sub + TPA, ntot - 1), nu, A.pmaxn)) : row.base;
 #pragma unroll 2
     for (int kk = sub; kk < ntot; kk += TPA) {
         float4 const pj = pn;
-        pn = A.posf[row.at(list_slot(min(kk + TPA, ntot - 1), nu, A.pmaxn))];
+        pn = A.posf[jn];
+        jn = row.at(list_slot(min(kk + 2 * TPA, ntot - 1), nu, A.pmaxn));
         float dx, dy, dz;
         float const r2 = min_image_f(pi, pj, L, iL, dx, dy, dz);
         float const idr = rsqrtf(r2);
@@ -342,6 +346,7 @@ __device__ __forceinline__ void force_row_mx(AtomsView const &A, TablesView cons
     int jn = row.at(slot(sub));
     float4 pn = A.posf[jn];
     float2 fn = A.dF2f[jn];
+    jn = row.at(slot(min(sub + TPA, n - 1)));
     // The body has no branch: a pair beyond the cutoff is evaluated and its terms are
     // replaced by zeros (the sums then gain +0 or -0, which changes no sum), and the next
     // partner is always prefetched (the last one again at the end of the row). Two
@@ -351,9 +356,9 @@ __device__ __forceinline__ void force_row_mx(AtomsView const &A, TablesView cons
     for (int kk = sub; kk < n; kk += TPA) {
         float4 const pj = pn;
         float2 const dFj2 = fn;
-        jn = row.at(slot(min(kk + TPA, n - 1)));
         pn = A.posf[jn];
         fn = A.dF2f[jn];
+        jn = row.at(slot(min(kk + 2 * TPA, n - 1)));
         float dx, dy, dz;
         float const r2 = min_image_f(in.pi, pj, in.L, in.iL, dx, dy, dz);
         bool const in_cut = !(r2 > T.fr_cut_sq);
